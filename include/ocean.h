@@ -1,0 +1,127 @@
+/*
+ * ocean.h — C ABI of the B200-native estimation-based SpGEMM (C = A·B, CSR, FP64).
+ *
+ * Every entry point is plain C: pointers, sizes and status codes, no C++ or torch
+ * types. Device pointers are CUDA device addresses on the current device; a
+ * `stream` argument is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   - somespgemm::SpGEMM::SpGEMM(const Config&)          kernels/SpGEMM.cuh:211
+ *   - somespgemm::SpGEMM::run(shared_ptr<cuCSR>, ...)    kernels/SpGEMM.cuh:213-338
+ *   - somespgemm::SpGEMM::get_stats()                    kernels/SpGEMM.cuh:340-342
+ *   - somespgemm::from_json(const json&, Config&)        src/Utils.cpp:8-37
+ *   - somespgemm::cuCSR / convert(cuCSR&, const CSR&)    include/CSR.h:35-51, src/CSR.cpp:226-250
+ *   - somespgemm::loadCSR(const char*)                   src/CSR.cpp:119-152
+ * Errors: the reference exits the process on CUDA errors (include/Common.h:296-310)
+ * and throws on capacity/config problems; here every call returns an ocean_status
+ * and ocean_last_error() gives the message of the calling thread's last failure.
+ */
+#ifndef OCEAN_H_
+#define OCEAN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  OCEAN_OK = 0,
+  OCEAN_ERR_CUDA = 1,      /* a CUDA runtime call or kernel launch failed */
+  OCEAN_ERR_CAPACITY = 2,  /* a bounded device structure (table, window, buffer) ran full */
+  OCEAN_ERR_TIMEOUT = 3,   /* a bounded device-side wait gave up */
+  OCEAN_ERR_INVALID = 4,   /* bad argument, dimension mismatch, bad config or file */
+  OCEAN_ERR_OOM = 5,       /* device or pinned host allocation failed */
+  OCEAN_ERR_INTERNAL = 6   /* an internal consistency check failed */
+} ocean_status;
+
+/* Read-only CSR view. `rowptr_bits` is 32 or 64. As in the reference
+ * (src/CSR.cpp:54), the end of the last row is taken from `nnz`, so
+ * rowptr[rows] is never read. Column ids are uint32, values double. */
+typedef struct {
+  uint64_t rows, cols, nnz;
+  const void* rowptr;
+  int32_t rowptr_bits;
+  const uint32_t* col;
+  const double* val;
+} ocean_csr_view;
+
+/* Owning CSR result. rowptr has rows+1 entries and rowptr[rows] == nnz (a
+ * superset of the reference's contract, which leaves the last offset unspecified).
+ * `rowptr_bits` is 32 when nnz < 2^32 (unless the config asks for 64), else 64.
+ * `location` is 0 for device memory (free with ocean_csr_free) and 1 for pinned
+ * host memory lent by the handle (valid until the next call on that handle). */
+typedef struct {
+  uint64_t rows, cols, nnz;
+  void* rowptr;
+  int32_t rowptr_bits;
+  uint32_t* col;
+  double* val;
+  int32_t location;
+  void* _owner; /* internal: allocation record */
+} ocean_csr;
+
+typedef struct ocean_handle ocean_handle;
+
+/* Create a handle from JSON config text (NULL or "" = defaults). Accepts every
+ * key of the reference's from_json (src/Utils.cpp:9-36, e.g. "track_stage_time",
+ * "use_estimation_workflow", "hll_numeric_malloc_expansion_coe",
+ * "segmentation_grid_max") with the same meaning, ignores unknown keys, and adds
+ * optional keys of its own ("output_rowptr_bits", "estimator", ...). */
+int ocean_create(ocean_handle** out, const char* json_config);
+/* Same, reading the JSON config from a file path (reference: src/main.cu:53-59). */
+int ocean_create_from_file(ocean_handle** out, const char* json_path);
+void ocean_destroy(ocean_handle* h);
+
+/* C = A·B with A, B in device memory. Allocates C on `stream` (stream-ordered
+ * pool) and returns with C complete on `stream`. Replaces SpGEMM::run. */
+int ocean_spgemm(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B,
+                 ocean_csr* C, void* stream);
+
+/* C = A·B with A, B in HOST memory (pinned or pageable). The call copies A and
+ * B to the device, multiplies, and copies C back into pinned host buffers owned
+ * by the handle (C->location == 1, reused by the next call). Replaces the
+ * reference driver's cuCSR(H2D) → run → CSR(D2H) sequence (src/main.cu:61-67). */
+int ocean_spgemm_host(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B,
+                      ocean_csr* C, void* stream);
+
+/* Release a device result of ocean_spgemm (stream-ordered on `stream`). */
+int ocean_csr_free(ocean_csr* C, void* stream);
+
+/* Copy a result into caller host buffers (rowptr: rows+1 entries of
+ * C->rowptr_bits, col/val: nnz entries) and wait for the copy. Replaces
+ * convert(CSR&, const cuCSR&) (src/CSR.cpp:243-250). */
+int ocean_csr_download(const ocean_csr* C, void* rowptr, uint32_t* col, double* val, void* stream);
+
+/* Exact per-row output counts of A·B (the symbolic phase alone) into the
+ * device array row_nnz[A.rows]. Replaces the symbolic kernels' result
+ * d_num_outputs_row (kernels/SpGEMM.cuh:759-923). */
+int ocean_symbolic(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B,
+                   uint32_t* row_nnz, void* stream);
+
+/* Stats of the last multiply as JSON text, with the reference's keys
+ * (kernels/SpGEMM.cuh:1788-1890: "A","B","C","stats","decision","timing",
+ * "total_time","gflops", ...). If cap is too small, *needed gets the size. */
+int ocean_stats_json(ocean_handle* h, char* buf, size_t cap, size_t* needed);
+
+/* Device time in milliseconds of the last call's named stage ("analysis",
+ * "symbolic", "scan", "numeric", "numeric_bitmap", ...), measured with CUDA
+ * events on the launching stream when "track_stage_time" is on; -1 if absent. */
+double ocean_stage_ms(ocean_handle* h, const char* stage);
+
+/* 32-bit MurmurHash3 of each uint32 key with the given seed, on the device
+ * (reference: kernels/MurmurHash.cuh:44-98, seed 1234 at include/Common.h:73). */
+int ocean_murmur3_u32(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed,
+                      void* stream);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* ocean_last_error(void);
+/* Library version string. */
+const char* ocean_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OCEAN_H_ */

@@ -1,0 +1,257 @@
+// Runtime configuration: the reference's JSON keys with the reference's defaults
+// (include/Utils.h:17-108, src/Utils.cpp:8-37), plus this library's own keys.
+// A small JSON reader is included; it keeps the top-level scalar members of an
+// object and skips nested values and unknown keys, like the reference's
+// assign_if_present (include/Utils.h:111-115).
+#pragma once
+#include <cctype>
+#include <cstdlib>
+#include <map>
+#include <stdexcept>
+#include <string>
+
+namespace ocean {
+
+struct JsonScalar {
+  enum Kind { kNull, kBool, kNumber, kString } kind = kNull;
+  bool b = false;
+  double num = 0.0;
+  std::string str;
+};
+
+class FlatJson {
+ public:
+  // Parses `text`; throws std::invalid_argument on malformed input.
+  static std::map<std::string, JsonScalar> parse(const std::string& text) {
+    FlatJson p(text);
+    std::map<std::string, JsonScalar> out;
+    p.ws();
+    if (p.i_ == p.s_.size()) return out;  // empty document = defaults
+    p.expect('{');
+    p.ws();
+    if (p.peek() == '}') {
+      ++p.i_;
+      return out;
+    }
+    for (;;) {
+      p.ws();
+      std::string key = p.string_lit();
+      p.ws();
+      p.expect(':');
+      p.ws();
+      JsonScalar v;
+      if (p.value(&v)) out[key] = v;
+      p.ws();
+      const char c = p.next();
+      if (c == '}') break;
+      if (c != ',') throw std::invalid_argument("config JSON: expected ',' or '}'");
+    }
+    return out;
+  }
+
+ private:
+  explicit FlatJson(const std::string& s) : s_(s) {}
+  const std::string& s_;
+  size_t i_ = 0;
+  char peek() const { return i_ < s_.size() ? s_[i_] : '\0'; }
+  char next() {
+    if (i_ >= s_.size()) throw std::invalid_argument("config JSON: unexpected end");
+    return s_[i_++];
+  }
+  void ws() {
+    while (i_ < s_.size() && std::isspace((unsigned char)s_[i_])) ++i_;
+  }
+  void expect(char c) {
+    if (next() != c) throw std::invalid_argument(std::string("config JSON: expected '") + c + "'");
+  }
+  std::string string_lit() {
+    expect('"');
+    std::string r;
+    for (;;) {
+      char c = next();
+      if (c == '"') break;
+      if (c == '\\') {
+        char e = next();
+        switch (e) {
+          case 'n': r += '\n'; break;
+          case 't': r += '\t'; break;
+          case 'r': r += '\r'; break;
+          case 'b': r += '\b'; break;
+          case 'f': r += '\f'; break;
+          case 'u': {
+            unsigned code = 0;
+            for (int k = 0; k < 4; ++k) {
+              const char h = next();
+              code = code * 16 + (std::isdigit((unsigned char)h) ? h - '0' : (std::tolower(h) - 'a' + 10));
+            }
+            r += code < 128 ? (char)code : '?';
+            break;
+          }
+          default: r += e;
+        }
+      } else {
+        r += c;
+      }
+    }
+    return r;
+  }
+  // Returns true for a scalar, false for a nested object/array (skipped).
+  bool value(JsonScalar* v) {
+    const char c = peek();
+    if (c == '"') {
+      v->kind = JsonScalar::kString;
+      v->str = string_lit();
+      return true;
+    }
+    if (c == '{' || c == '[') {
+      skip_nested();
+      return false;
+    }
+    if (s_.compare(i_, 4, "true") == 0) {
+      i_ += 4;
+      v->kind = JsonScalar::kBool;
+      v->b = true;
+      return true;
+    }
+    if (s_.compare(i_, 5, "false") == 0) {
+      i_ += 5;
+      v->kind = JsonScalar::kBool;
+      v->b = false;
+      return true;
+    }
+    if (s_.compare(i_, 4, "null") == 0) {
+      i_ += 4;
+      v->kind = JsonScalar::kNull;
+      return true;
+    }
+    const char* start = s_.c_str() + i_;
+    char* end = nullptr;
+    const double d = std::strtod(start, &end);
+    if (end == start) throw std::invalid_argument("config JSON: bad value");
+    i_ += (size_t)(end - start);
+    v->kind = JsonScalar::kNumber;
+    v->num = d;
+    return true;
+  }
+  void skip_nested() {
+    int depth = 0;
+    do {
+      const char c = next();
+      if (c == '"') {
+        --i_;
+        string_lit();
+        continue;
+      }
+      if (c == '{' || c == '[') ++depth;
+      if (c == '}' || c == ']') --depth;
+    } while (depth > 0);
+  }
+};
+
+struct Config {
+  // reference keys (src/Utils.cpp:9-36) with reference defaults (include/Utils.h)
+  bool track_stage_times = false;
+  bool check_correctness = false;
+  bool output_stats = false;
+  double compare_relative_error = 1e-6;
+  double compare_autofail_relative_error = 1e-4;
+  std::string ground_truth_file;
+  std::string stats_output_file;
+  int warmup_iters = 10, bench_iters = 10;
+  bool print_info = false;
+  bool print_memory = false;
+  bool use_estimation_workflow = true;
+  bool use_ultrasparse_workflow = true;
+  bool use_assist_information = true;
+  bool use_hybrid_accumulator = true;
+  bool use_indirect_sort = true;
+  bool use_fat_workflow = true;
+  double hll_numeric_malloc_expansion_coe = 1.3;
+  int estimation_input_expansion_threshold = 8;
+  int estimation_output_compaction_threshold = 8;
+  bool use_segmented_workflow = false;
+  int segmentation_grid_max = 256;
+  double segmentation_hot_threshold_k = 2.0;
+  int segmentation_min_segment_rows = 1024;
+  int segmentation_cc_max_iters = 32;
+  // code-only reference defaults (include/Utils.h:36-60)
+  int usparse_avg_product_threshold = 64;
+  double hll_sample_rate = 0.03;
+  int hll_sample_min_rows = 648;
+  int hll_sample_max_rows = 10800;
+  int hll_higher_precision_expansion_threshold = 48;
+  // this library's keys
+  int output_rowptr_bits = 0;     // 0: 32 when nnz(C) < 2^32, else 64
+  int esc_max_products = 32;      // rows with at most this many products use the ESC class
+  int force_sym_bin = -1;         // testing: put every non-empty row in one symbolic class
+  int force_num_bin = -1;         // testing: put every non-empty row in one numeric class
+  bool sync_on_return = true;     // check device status before returning
+
+  static Config from_json_text(const std::string& text) {
+    Config c;
+    const auto m = FlatJson::parse(text);
+    auto getb = [&](const char* k, bool& f) {
+      auto it = m.find(k);
+      if (it == m.end()) return;
+      if (it->second.kind == JsonScalar::kBool) f = it->second.b;
+      else if (it->second.kind == JsonScalar::kNumber) f = it->second.num != 0.0;
+      else throw std::invalid_argument(std::string("config key '") + k + "' must be a boolean");
+    };
+    auto getd = [&](const char* k, double& f) {
+      auto it = m.find(k);
+      if (it == m.end()) return;
+      if (it->second.kind != JsonScalar::kNumber)
+        throw std::invalid_argument(std::string("config key '") + k + "' must be a number");
+      f = it->second.num;
+    };
+    auto geti = [&](const char* k, int& f) {
+      double d = f;
+      getd(k, d);
+      f = (int)d;
+    };
+    auto gets = [&](const char* k, std::string& f) {
+      auto it = m.find(k);
+      if (it == m.end()) return;
+      if (it->second.kind != JsonScalar::kString)
+        throw std::invalid_argument(std::string("config key '") + k + "' must be a string");
+      f = it->second.str;
+    };
+    getb("track_stage_time", c.track_stage_times);
+    getb("check_correctness", c.check_correctness);
+    getb("output_stats", c.output_stats);
+    getd("compare_relative_error", c.compare_relative_error);
+    getd("compare_autofail_relative_error", c.compare_autofail_relative_error);
+    gets("ground_truth_file", c.ground_truth_file);
+    gets("stats_output_file", c.stats_output_file);
+    geti("warmup_iters", c.warmup_iters);
+    geti("bench_iters", c.bench_iters);
+    getb("print_info", c.print_info);
+    getb("print_memory", c.print_memory);
+    getb("use_estimation_workflow", c.use_estimation_workflow);
+    getb("use_ultrasparse_workflow", c.use_ultrasparse_workflow);
+    getb("use_assist_information", c.use_assist_information);
+    getb("use_hybrid_accumulator", c.use_hybrid_accumulator);
+    getb("use_indirect_sort", c.use_indirect_sort);
+    getb("use_fat_workflow", c.use_fat_workflow);
+    getd("hll_numeric_malloc_expansion_coe", c.hll_numeric_malloc_expansion_coe);
+    geti("estimation_input_expansion_threshold", c.estimation_input_expansion_threshold);
+    geti("estimation_output_compaction_threshold", c.estimation_output_compaction_threshold);
+    getb("use_segmented_workflow", c.use_segmented_workflow);
+    geti("segmentation_grid_max", c.segmentation_grid_max);
+    getd("segmentation_hot_threshold_k", c.segmentation_hot_threshold_k);
+    geti("segmentation_min_segment_rows", c.segmentation_min_segment_rows);
+    geti("segmentation_cc_max_iters", c.segmentation_cc_max_iters);
+    geti("output_rowptr_bits", c.output_rowptr_bits);
+    geti("esc_max_products", c.esc_max_products);
+    geti("force_sym_bin", c.force_sym_bin);
+    geti("force_num_bin", c.force_num_bin);
+    getb("sync_on_return", c.sync_on_return);
+    if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
+      throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
+    if (c.esc_max_products < 0 || c.esc_max_products > 32)
+      throw std::invalid_argument("esc_max_products must be in [0, 32]");
+    return c;
+  }
+};
+
+}  // namespace ocean

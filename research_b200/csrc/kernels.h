@@ -1,0 +1,55 @@
+// Host-side launchers of the SpGEMM kernels (implemented in kernels_core.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "ocean_internal.cuh"
+
+namespace ocean {
+
+// Device buffers of one multiply, sized for `rows` rows of A.
+struct DevWork {
+  uint64_t rows = 0;
+  uint32_t* prod = nullptr;      // products per row (saturated to u32)
+  uint32_t* lo = nullptr;        // smallest output column per row (kEmpty if none)
+  uint32_t* hi = nullptr;        // largest output column per row
+  uint32_t* row_nnz = nullptr;   // exact output count per row
+  uint32_t* sym_bins = nullptr;  // [SB_COUNT][rows] row ids per symbolic class
+  uint32_t* num_bins = nullptr;  // [NB_COUNT][rows] row ids per numeric class
+  unsigned long long* tile_sums = nullptr;
+  uint64_t* rowptr64 = nullptr;  // rows+1 exclusive scan of row_nnz
+  uint32_t* rowptr32 = nullptr;  // same, truncated to 32 bits
+  DevCounters* ctr = nullptr;
+};
+
+constexpr int kScanTile = 4096;
+inline uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+struct SymPolicy {
+  uint32_t esc_max_products = 32;
+  int force_bin = -1;   // >= 0: every non-empty row goes to this class (tests)
+};
+struct NumPolicy {
+  uint32_t esc_max_products = 32;
+  int force_bin = -1;
+};
+
+template <typename RP>
+void launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
+                     cudaStream_t s);
+
+template <typename RP>
+void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms,
+                     cudaStream_t s);
+
+void launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s);
+
+template <typename RP>
+void launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_t* c_col,
+                    double* c_val, int num_sms, cudaStream_t s, cudaEvent_t* bin_events);
+
+void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, cudaStream_t s);
+
+// Per-kernel dynamic shared memory opt-in; call once per device.
+void configure_kernel_attributes();
+
+}  // namespace ocean

@@ -1,0 +1,881 @@
+// SpGEMM kernels for sm_100a: row analysis, symbolic and numeric accumulators, scan.
+//
+// Reference counterparts (paths inside the reference project):
+//   row analysis            kernels/Analysis.cuh:31-105   (analysisKernel)
+//   row binning             kernels/Analysis.cuh:110-303  (binning / numericBinning)
+//   ESC accumulator         kernels/AccumulatorESC.cuh:12-166
+//   hash accumulators       kernels/AccumulatorHash.cuh:11-755, kernels/Hashmap.cuh:14-281
+//   dense accumulators      kernels/AccumulatorDense.cuh:43-893
+//   row-pointer scan        cub::DeviceScan::ExclusiveSum at kernels/SpGEMM.cuh:1147,1221,1622
+//   column sort             kernels/Epilogue.cuh:68-222 (CUB BlockRadixSort)
+//
+// Design: every row class runs as a persistent kernel whose blocks pull rows
+// from a device-side class list, so no bin count is read back to the host. The
+// only host read-back of a multiply is the total output count (to allocate C).
+// Numeric kernels write each row already sorted straight into its final place
+// in C, so there is no temporary output buffer and no separate sort/copy pass.
+#include <cstdio>
+#include "kernels.h"
+
+namespace ocean {
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Block-wide sum; `scratch` holds 33 entries. All threads get the result.
+template <int NT>
+__device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v,
+                                                            unsigned long long* scratch) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  v = warp_sum_u64(v);
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned long long t = lane < NT / 32 ? scratch[lane] : 0ull;
+    t = warp_sum_u64(t);
+    if (lane == 0) scratch[32] = t;
+  }
+  __syncthreads();
+  const unsigned long long r = scratch[32];
+  __syncthreads();
+  return r;
+}
+
+// Block-wide exclusive scan; `scratch` holds 33 entries; *total gets the sum.
+template <int NT, typename T>
+__device__ __forceinline__ T block_excl_scan(T v, T* scratch, T* total) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) scratch[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const T s = lane < NT / 32 ? scratch[lane] : T(0);
+    T incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane < NT / 32) scratch[lane] = incl - s;
+    if (lane == 31) scratch[32] = incl;
+  }
+  __syncthreads();
+  const T r = scratch[warp] + x - v;
+  *total = scratch[32];
+  __syncthreads();
+  return r;
+}
+
+__device__ __forceinline__ void raise_status(DevCounters* ctr, unsigned bit, uint32_t row) {
+  const unsigned old = atomicOr(&ctr->status, bit);
+  if (old == 0) ctr->err_row = row;
+}
+
+// Symbolic class of a row from its product count and output column span.
+__device__ __forceinline__ int sym_bin_for(uint64_t p, uint64_t span, const SymPolicy& pol) {
+  if (pol.force_bin >= 0) return pol.force_bin;
+  if (p <= pol.esc_max_products) return SB_ESC;
+  const uint64_t words = (span + 63) >> 6;
+  if (p > 16384) return SB_BITMAP;
+  if (p <= 1024) return SB_HASH_S;
+  if (p <= 4096) return (words <= 2048) ? SB_BITMAP : SB_HASH_M;
+  return (words <= 8192) ? SB_BITMAP : SB_HASH_L;
+}
+
+// Numeric class of a row from its exact output count.
+__device__ __forceinline__ int num_bin_for(uint32_t n, uint64_t p, uint64_t span,
+                                           const NumPolicy& pol) {
+  if (n == 0) return -1;
+  if (pol.force_bin >= 0) return pol.force_bin;
+  if (p <= pol.esc_max_products) return NB_ESC;
+  const uint64_t words = (span + 63) >> 6;
+  if (n <= 512) return NB_HASH_S;
+  if (n <= 2048) return (words <= 1024) ? NB_BITMAP : NB_HASH_M;
+  if (n <= 4096) return (words <= 4096) ? NB_BITMAP : NB_HASH_L;
+  return NB_BITMAP;
+}
+
+// ---------------------------------------------------------------- analysis
+// One group of G lanes per row of A: products, output column span; then the
+// row is appended to its symbolic class list (rows with no product get
+// row_nnz = 0 here and no class).
+template <typename RP, int G>
+__global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
+                                                  uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
+                                                  uint32_t* __restrict__ row_nnz,
+                                                  uint32_t* __restrict__ sym_bins,
+                                                  DevCounters* __restrict__ ctr, SymPolicy pol) {
+  const int lane = threadIdx.x & 31;
+  const int sl = lane & (G - 1);
+  const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool valid = row < A.rows;
+  uint64_t a0 = 0, a1 = 0;
+  if (valid) {
+    a0 = A.row_begin(row);
+    a1 = A.row_end(row);
+  }
+  unsigned long long p = 0;
+  uint32_t mn = kEmpty, mx = 0;
+  for (uint64_t k = a0 + sl; k < a1; k += G) {
+    const uint32_t j = A.col[k];
+    const uint64_t b0 = B.row_begin(j), b1 = B.row_end(j);
+    if (b1 > b0) {
+      p += b1 - b0;
+      mn = min(mn, B.col[b0]);
+      mx = max(mx, B.col[b1 - 1]);
+    }
+  }
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    p += __shfl_xor_sync(kFull, p, o);
+    mn = min(mn, __shfl_xor_sync(kFull, mn, o));
+    mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+  }
+  int b = -1;
+  const bool leader = valid && sl == 0;
+  if (leader) {
+    prod[row] = p > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)p;
+    lo[row] = mn;
+    hi[row] = mx;
+    if (p == 0) {
+      row_nnz[row] = 0;
+    } else {
+      b = sym_bin_for(p, (uint64_t)mx - mn + 1, pol);
+    }
+  }
+  bin_append(b, (uint32_t)row, ctr->sym_count, sym_bins, A.rows);
+  // totals for stats and the workflow decision
+  unsigned long long tp = leader ? p : 0ull;
+  tp = warp_sum_u64(tp);
+  unsigned mp = leader ? (p > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned)p) : 0u;
+  unsigned ma = leader ? (unsigned)(a1 - a0) : 0u;
+  mp = __reduce_max_sync(kFull, mp);
+  ma = __reduce_max_sync(kFull, ma);
+  if (lane == 0) {
+    if (tp) atomicAdd(&ctr->total_products, tp);
+    if (mp) atomicMax(&ctr->max_products, mp);
+    if (ma) atomicMax(&ctr->max_a_nnz, ma);
+  }
+}
+
+// ---------------------------------------------------------------- ESC (<= 32 products)
+// Lists the (<= 32) products of `row` in warp order: src[i] = index into B,
+// aidx[i] = index into A. Returns the product count.
+template <typename RP>
+__device__ __forceinline__ uint32_t gather_products(const Csr<RP>& A, const Csr<RP>& B, uint32_t row,
+                                                    uint64_t* src, uint64_t* aidx) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+  uint32_t base = 0;
+  for (uint64_t k0 = a0; k0 < a1; k0 += 32) {
+    const uint64_t k = k0 + lane;
+    uint64_t b0 = 0;
+    uint32_t len = 0;
+    if (k < a1) {
+      const uint32_t j = A.col[k];
+      b0 = B.row_begin(j);
+      const uint64_t l = B.row_end(j) - b0;
+      len = l > 64 ? 64u : (uint32_t)l;
+    }
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t excl = base + incl - len;
+    for (uint32_t t = 0; t < len && excl + t < 32; ++t) {
+      src[excl + t] = b0 + t;
+      if (aidx) aidx[excl + t] = k;
+    }
+    base += __shfl_sync(kFull, incl, 31);
+  }
+  __syncwarp();
+  return base;
+}
+
+template <typename RP>
+__global__ void __launch_bounds__(256) k_sym_esc(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
+                                                 DevCounters* __restrict__ ctr,
+                                                 uint32_t* __restrict__ row_nnz) {
+  __shared__ uint64_t s_src[8][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t count = ctr->sym_count[SB_ESC];
+  const uint32_t* list = bins + (uint64_t)SB_ESC * A.rows;
+  for (uint64_t idx = (uint64_t)blockIdx.x * 8 + warp; idx < count; idx += (uint64_t)gridDim.x * 8) {
+    const uint32_t row = list[idx];
+    const uint32_t np = gather_products(A, B, row, s_src[warp], nullptr);
+    if (np > 32 && lane == 0) raise_status(ctr, DEV_BIN_OVERFLOW, row);
+    const uint32_t col = lane < np ? B.col[s_src[warp][lane]] : kEmpty;
+    const unsigned peers = __match_any_sync(kFull, col);
+    const bool first = (col != kEmpty) && (__ffs(peers) - 1 == lane);
+    const unsigned n = __popc(__ballot_sync(kFull, first));
+    if (lane == 0) row_nnz[row] = n;
+    __syncwarp();
+  }
+}
+
+// Numeric ESC: one product per lane, 32-lane bitonic sort by column in
+// registers, segmented suffix sum, ordered write of the distinct columns.
+template <typename RP>
+__global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
+                                                 DevCounters* __restrict__ ctr,
+                                                 const uint32_t* __restrict__ row_nnz,
+                                                 const uint64_t* __restrict__ rowptr,
+                                                 uint32_t* __restrict__ c_col, double* __restrict__ c_val) {
+  __shared__ uint64_t s_src[8][32];
+  __shared__ uint64_t s_aidx[8][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t count = ctr->num_count[NB_ESC];
+  const uint32_t* list = bins + (uint64_t)NB_ESC * A.rows;
+  for (uint64_t idx = (uint64_t)blockIdx.x * 8 + warp; idx < count; idx += (uint64_t)gridDim.x * 8) {
+    const uint32_t row = list[idx];
+    const uint32_t np = gather_products(A, B, row, s_src[warp], s_aidx[warp]);
+    if (np > 32 && lane == 0) raise_status(ctr, DEV_BIN_OVERFLOW, row);
+    uint32_t key = kEmpty;
+    double v = 0.0;
+    if (lane < np) {
+      const uint64_t s = s_src[warp][lane];
+      key = B.col[s];
+      v = A.val[s_aidx[warp][lane]] * B.val[s];
+    }
+    // bitonic sort of 32 (key, value) pairs across lanes, ascending
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        const uint32_t ok = __shfl_xor_sync(kFull, key, j);
+        const double ov = __shfl_xor_sync(kFull, v, j);
+        const bool asc = (lane & k) == 0;
+        const bool low = (lane & j) == 0;
+        const bool take = (low == asc) ? (ok < key) : (ok > key);
+        if (take) {
+          key = ok;
+          v = ov;
+        }
+      }
+    }
+    // segmented suffix sum: lanes holding the same column are adjacent
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t ck = __shfl_down_sync(kFull, key, d);
+      const double cv = __shfl_down_sync(kFull, v, d);
+      if (lane + d < 32 && ck == key) v += cv;
+    }
+    const uint32_t prev = __shfl_up_sync(kFull, key, 1);
+    const bool head = key != kEmpty && (lane == 0 || prev != key);
+    const unsigned heads = __ballot_sync(kFull, head);
+    const uint32_t n = __popc(heads);
+    const uint32_t expect = row_nnz[row];
+    if (n != expect && lane == 0) raise_status(ctr, DEV_COUNT_MISMATCH, row);
+    const uint32_t pos = __popc(heads & lanemask_lt());
+    if (head && pos < expect) {
+      const uint64_t off = rowptr[row] + pos;
+      c_col[off] = key;
+      c_val[off] = v;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- hash accumulators
+// Symbolic: one block per row, open-addressing set of column ids in shared memory
+// (linear probing, bounded by the table size).
+template <typename RP, int NT, int LOG2T>
+__global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
+                                                 DevCounters* __restrict__ ctr, int bin,
+                                                 const uint32_t* __restrict__ prod,
+                                                 uint32_t* __restrict__ row_nnz) {
+  constexpr int T = 1 << LOG2T;
+  extern __shared__ uint32_t keys[];
+  __shared__ unsigned long long red[33];
+  __shared__ uint32_t s_idx;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < T; i += NT) keys[i] = kEmpty;
+  const uint32_t count = ctr->sym_count[bin];
+  const uint32_t* list = bins + (uint64_t)bin * A.rows;
+  for (;;) {
+    if (tid == 0) s_idx = atomicAdd(&ctr->sym_cursor[bin], 1u);
+    __syncthreads();
+    const uint32_t idx = s_idx;
+    if (idx >= count) break;
+    const uint32_t row = list[idx];
+    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+    const int g = group_size_for(prod[row], a1 - a0);
+    const int gid = tid / g, gl = tid % g, ngr = NT / g;
+    unsigned cnt = 0;
+    bool full = false;
+    for (uint64_t k = a0 + gid; k < a1; k += ngr) {
+      const uint32_t j = A.col[k];
+      const uint64_t b1 = B.row_end(j);
+      for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
+        const uint32_t c = B.col[q];
+        uint32_t h = hash_slot(c, LOG2T);
+        int probe = 0;
+        for (; probe < T; ++probe) {
+          const uint32_t cur = keys[h];
+          if (cur == c) break;
+          if (cur == kEmpty) {
+            const uint32_t prev = atomicCAS(&keys[h], kEmpty, c);
+            if (prev == kEmpty) {
+              ++cnt;
+              break;
+            }
+            if (prev == c) break;
+          }
+          h = (h + 1) & (T - 1);
+        }
+        full |= probe == T;
+      }
+    }
+    if (full) raise_status(ctr, DEV_TABLE_FULL, row);
+    const unsigned long long total = block_sum_u64<NT>(cnt, red);
+    if (tid == 0) row_nnz[row] = (uint32_t)total;
+    for (int i = tid; i < T; i += NT) keys[i] = kEmpty;
+  }
+}
+
+// Numeric: hash-accumulate FP64 values in shared memory, compact the occupied
+// slots into (column << 32 | slot) keys, bitonic-sort them in shared memory and
+// write the row in column order directly into C.
+template <typename RP, int NT, int LOG2T>
+__global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
+                                                 DevCounters* __restrict__ ctr, int bin,
+                                                 const uint32_t* __restrict__ prod,
+                                                 const uint32_t* __restrict__ row_nnz,
+                                                 const uint64_t* __restrict__ rowptr,
+                                                 uint32_t* __restrict__ c_col, double* __restrict__ c_val) {
+  constexpr int T = 1 << LOG2T;
+  constexpr int PER = T / NT;
+  constexpr int CAP = T / 2;  // sort capacity (entries) in the reused key area
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* vals = reinterpret_cast<double*>(smem_raw);
+  uint32_t* keys = reinterpret_cast<uint32_t*>(vals + T);
+  unsigned long long* sortbuf = reinterpret_cast<unsigned long long*>(keys);
+  __shared__ uint32_t s_idx, s_n;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < T; i += NT) {
+    keys[i] = kEmpty;
+    vals[i] = 0.0;
+  }
+  const uint32_t count = ctr->num_count[bin];
+  const uint32_t* list = bins + (uint64_t)bin * A.rows;
+  for (;;) {
+    if (tid == 0) {
+      s_idx = atomicAdd(&ctr->num_cursor[bin], 1u);
+      s_n = 0;
+    }
+    __syncthreads();
+    const uint32_t idx = s_idx;
+    if (idx >= count) break;
+    const uint32_t row = list[idx];
+    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+    const int g = group_size_for(prod[row], a1 - a0);
+    const int gid = tid / g, gl = tid % g, ngr = NT / g;
+    bool full = false;
+    for (uint64_t k = a0 + gid; k < a1; k += ngr) {
+      const uint32_t j = A.col[k];
+      const double av = A.val[k];
+      const uint64_t b1 = B.row_end(j);
+      for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
+        const uint32_t c = B.col[q];
+        const double v = av * B.val[q];
+        uint32_t h = hash_slot(c, LOG2T);
+        int probe = 0;
+        for (; probe < T; ++probe) {
+          const uint32_t cur = keys[h];
+          if (cur == c) {
+            atomicAdd(&vals[h], v);
+            break;
+          }
+          if (cur == kEmpty) {
+            const uint32_t prev = atomicCAS(&keys[h], kEmpty, c);
+            if (prev == kEmpty || prev == c) {
+              atomicAdd(&vals[h], v);
+              break;
+            }
+          }
+          h = (h + 1) & (T - 1);
+        }
+        full |= probe == T;
+      }
+    }
+    if (full) raise_status(ctr, DEV_TABLE_FULL, row);
+    __syncthreads();
+    // compaction: read this thread's slots, then rewrite the key area as sort keys
+    uint32_t mine[PER];
+    unsigned cnt = 0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      mine[i] = keys[tid + i * NT];
+      cnt += mine[i] != kEmpty;
+    }
+    const unsigned base = cnt ? atomicAdd(&s_n, cnt) : 0u;
+    __syncthreads();
+    const uint32_t n = s_n;
+    if (n <= CAP) {
+      unsigned w = base;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        if (mine[i] != kEmpty)
+          sortbuf[w++] = ((unsigned long long)mine[i] << 32) | (unsigned)(tid + i * NT);
+      }
+    }
+    uint32_t np2 = 1;
+    while (np2 < n) np2 <<= 1;
+    if (np2 > CAP) np2 = CAP;
+    for (uint32_t i = n + tid; i < np2; i += NT) sortbuf[i] = ~0ull;
+    __syncthreads();
+    // bitonic sort of np2 keys
+    for (uint32_t k = 2; k <= np2; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = tid; i < np2 / 2; i += NT) {
+          const uint32_t l = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+          const uint32_t r = l + j;
+          const unsigned long long x = sortbuf[l], y = sortbuf[r];
+          const bool asc = (l & k) == 0;
+          if ((x > y) == asc) {
+            sortbuf[l] = y;
+            sortbuf[r] = x;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    const uint32_t expect = row_nnz[row];
+    if (tid == 0 && (n != expect || n > CAP)) raise_status(ctr, DEV_COUNT_MISMATCH, row);
+    // rows that overflowed the sort capacity were not compacted: write nothing
+    const uint32_t wn = (n <= CAP) ? min(n, expect) : 0u;
+    const uint64_t off = rowptr[row];
+    for (uint32_t i = tid; i < wn; i += NT) {
+      const unsigned long long e = sortbuf[i];
+      c_col[off + i] = (uint32_t)(e >> 32);
+      c_val[off + i] = vals[(uint32_t)e];
+    }
+    __syncthreads();
+    for (int i = tid; i < T; i += NT) {
+      keys[i] = kEmpty;
+      vals[i] = 0.0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- bitmap accumulators
+// Symbolic: a bitmap over (a window of) the row's output column span; the count
+// is the popcount. Windows of 2^20 columns sweep wider spans.
+template <typename RP>
+__global__ void __launch_bounds__(kBitmapThreads, 1)
+    k_sym_bitmap(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins, DevCounters* __restrict__ ctr,
+                 const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
+                 const uint32_t* __restrict__ hi, uint32_t* __restrict__ row_nnz) {
+  extern __shared__ unsigned long long bits[];
+  __shared__ unsigned long long red[33];
+  __shared__ uint32_t s_idx;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kBitmapWords; i += kBitmapThreads) bits[i] = 0ull;
+  const uint32_t count = ctr->sym_count[SB_BITMAP];
+  const uint32_t* list = bins + (uint64_t)SB_BITMAP * A.rows;
+  for (;;) {
+    if (tid == 0) s_idx = atomicAdd(&ctr->sym_cursor[SB_BITMAP], 1u);
+    __syncthreads();
+    const uint32_t idx = s_idx;
+    if (idx >= count) break;
+    const uint32_t row = list[idx];
+    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+    const int g = group_size_for(prod[row], a1 - a0);
+    const int gid = tid / g, gl = tid % g, ngr = kBitmapThreads / g;
+    const uint64_t rlo = lo[row], rhi = hi[row];
+    unsigned long long total = 0;
+    for (uint64_t w0 = rlo; w0 <= rhi; w0 += kBitmapBits) {
+      const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
+      const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
+      for (uint64_t k = a0 + gid; k < a1; k += ngr) {
+        const uint32_t j = A.col[k];
+        const uint64_t b1 = B.row_end(j);
+        for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
+          const uint64_t c = B.col[q];
+          if (c >= w0 && c < w1) {
+            const uint32_t d = (uint32_t)(c - w0);
+            atomicOr(&bits[d >> 6], 1ull << (d & 63));
+          }
+        }
+      }
+      __syncthreads();
+      unsigned long long cnt = 0;
+      for (uint32_t w = tid; w < nwords; w += kBitmapThreads) {
+        cnt += __popcll(bits[w]);
+        bits[w] = 0ull;
+      }
+      total += block_sum_u64<kBitmapThreads>(cnt, red);
+    }
+    if (tid == 0) row_nnz[row] = (uint32_t)total;
+  }
+}
+
+// Numeric: bitmap-rank accumulator. Pass 1 marks the output columns of the
+// window; a block scan turns the bitmap into a rank table (u16 word offsets
+// inside 1024-word superblocks plus u32 superblock offsets); the sorted column
+// ids are written from the bitmap and the values are accumulated straight into
+// C at position rank(column) with FP64 reductions in L2. Output is sorted by
+// construction; no hash collisions, no sort.
+struct BitmapNumSmem {
+  unsigned long long bits[kBitmapWords];
+  uint16_t wpre[kBitmapWords];
+  uint32_t spre[kSupers];
+  uint32_t scan[33];
+  uint32_t s_idx;
+};
+
+template <typename RP>
+__global__ void __launch_bounds__(kBitmapThreads, 1)
+    k_num_bitmap(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins, DevCounters* __restrict__ ctr,
+                 const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
+                 const uint32_t* __restrict__ hi, const uint32_t* __restrict__ row_nnz,
+                 const uint64_t* __restrict__ rowptr, uint32_t* __restrict__ c_col,
+                 double* __restrict__ c_val) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BitmapNumSmem& S = *reinterpret_cast<BitmapNumSmem*>(smem_raw);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kBitmapWords; i += kBitmapThreads) S.bits[i] = 0ull;
+  const uint32_t count = ctr->num_count[NB_BITMAP];
+  const uint32_t* list = bins + (uint64_t)NB_BITMAP * A.rows;
+  for (;;) {
+    if (tid == 0) S.s_idx = atomicAdd(&ctr->num_cursor[NB_BITMAP], 1u);
+    __syncthreads();
+    const uint32_t idx = S.s_idx;
+    if (idx >= count) break;
+    const uint32_t row = list[idx];
+    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+    const int g = group_size_for(prod[row], a1 - a0);
+    const int gid = tid / g, gl = tid % g, ngr = kBitmapThreads / g;
+    const uint64_t rlo = lo[row], rhi = hi[row];
+    const uint64_t row_off = rowptr[row];
+    const uint32_t expect = row_nnz[row];
+    const uint64_t row_lim = row_off + expect;
+    uint64_t off = row_off;
+    for (uint64_t w0 = rlo; w0 <= rhi; w0 += kBitmapBits) {
+      const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
+      const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
+      // pass 1: mark columns
+      for (uint64_t k = a0 + gid; k < a1; k += ngr) {
+        const uint32_t j = A.col[k];
+        const uint64_t b1 = B.row_end(j);
+        for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
+          const uint64_t c = B.col[q];
+          if (c >= w0 && c < w1) {
+            const uint32_t d = (uint32_t)(c - w0);
+            atomicOr(&S.bits[d >> 6], 1ull << (d & 63));
+          }
+        }
+      }
+      __syncthreads();
+      // rank table: thread t owns words [16t, 16t+16)
+      const uint32_t wbeg = (uint32_t)tid * kWordsPerThread;
+      uint32_t local = 0;
+#pragma unroll
+      for (int i = 0; i < kWordsPerThread; ++i) {
+        const uint32_t w = wbeg + i;
+        local += (w < nwords) ? __popcll(S.bits[w]) : 0u;
+      }
+      uint32_t nw_total;
+      const uint32_t tpre = block_excl_scan<kBitmapThreads, uint32_t>(local, S.scan, &nw_total);
+      if ((tid & 63) == 0) S.spre[tid >> 6] = tpre;
+      __syncthreads();
+      {
+        const uint32_t sp = S.spre[tid >> 6];
+        uint32_t run = tpre;
+#pragma unroll 4
+        for (int i = 0; i < kWordsPerThread; ++i) {
+          const uint32_t w = wbeg + i;
+          if (w >= nwords) break;
+          unsigned long long word = S.bits[w];
+          S.wpre[w] = (uint16_t)(run - sp);
+          // sorted column ids of this word
+          while (word) {
+            const int bpos = __ffsll((long long)word) - 1;
+            word &= word - 1;
+            const uint64_t o = off + run;
+            if (o < row_lim) c_col[o] = (uint32_t)(w0 + (uint64_t)w * 64 + bpos);
+            ++run;
+          }
+        }
+      }
+      for (uint32_t i = tid; i < nw_total; i += kBitmapThreads) {
+        if (off + i < row_lim) c_val[off + i] = 0.0;
+      }
+      __syncthreads();
+      // pass 2: accumulate values at their ranks
+      for (uint64_t k = a0 + gid; k < a1; k += ngr) {
+        const uint32_t j = A.col[k];
+        const double av = A.val[k];
+        const uint64_t b1 = B.row_end(j);
+        for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
+          const uint64_t c = B.col[q];
+          if (c >= w0 && c < w1) {
+            const uint32_t d = (uint32_t)(c - w0);
+            const uint32_t w = d >> 6;
+            const uint32_t r = S.spre[w >> 10] + S.wpre[w] +
+                               __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));
+            if (off + r < row_lim) atomicAdd(&c_val[off + r], av * B.val[q]);
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < kWordsPerThread; ++i) {
+        const uint32_t w = wbeg + i;
+        if (w < nwords) S.bits[w] = 0ull;
+      }
+      off += nw_total;
+      __syncthreads();
+    }
+    if (tid == 0 && off != row_lim) raise_status(ctr, DEV_COUNT_MISMATCH, row);
+  }
+}
+
+// ---------------------------------------------------------------- scan
+__global__ void __launch_bounds__(1024) k_scan_reduce(const uint32_t* __restrict__ in, uint64_t n,
+                                                      unsigned long long* __restrict__ tile_sums) {
+  __shared__ unsigned long long red[33];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+  unsigned long long s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanTile / 1024; ++q) {
+    const uint64_t i = base + (uint64_t)q * 1024 + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  s = block_sum_u64<1024>(s, red);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(unsigned long long* __restrict__ tile_sums,
+                                                     uint64_t ntiles, DevCounters* __restrict__ ctr,
+                                                     uint64_t* __restrict__ rowptr64,
+                                                     uint32_t* __restrict__ rowptr32, uint64_t rows) {
+  __shared__ unsigned long long scr[33];
+  const uint64_t per = (ntiles + 1023) / 1024;
+  const uint64_t b = (uint64_t)threadIdx.x * per;
+  unsigned long long s = 0;
+  for (uint64_t i = 0; i < per; ++i)
+    if (b + i < ntiles) s += tile_sums[b + i];
+  unsigned long long total;
+  unsigned long long run = block_excl_scan<1024, unsigned long long>(s, scr, &total);
+  for (uint64_t i = 0; i < per; ++i) {
+    if (b + i < ntiles) {
+      const unsigned long long t = tile_sums[b + i];
+      tile_sums[b + i] = run;
+      run += t;
+    }
+  }
+  if (threadIdx.x == 0) {
+    ctr->total_nnz = total;
+    rowptr64[rows] = total;
+    rowptr32[rows] = (uint32_t)total;
+  }
+}
+
+// Per tile: local exclusive scan + tile offset -> row pointers; each row is
+// also appended to its numeric class list.
+__global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict__ in, uint64_t n,
+                                                     const unsigned long long* __restrict__ tile_offs,
+                                                     uint64_t* __restrict__ rowptr64,
+                                                     uint32_t* __restrict__ rowptr32,
+                                                     const uint32_t* __restrict__ prod,
+                                                     const uint32_t* __restrict__ lo,
+                                                     const uint32_t* __restrict__ hi,
+                                                     uint32_t* __restrict__ num_bins,
+                                                     DevCounters* __restrict__ ctr, NumPolicy pol) {
+  __shared__ unsigned long long scr[33];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * 4;
+  uint32_t v[4];
+  unsigned long long s = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    v[q] = (base + q < n) ? in[base + q] : 0u;
+    s += v[q];
+  }
+  unsigned long long total;
+  unsigned long long run = block_excl_scan<1024, unsigned long long>(s, scr, &total) + tile_offs[blockIdx.x];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint64_t i = base + q;
+    int b = -1;
+    if (i < n) {
+      rowptr64[i] = run;
+      rowptr32[i] = (uint32_t)run;
+      run += v[q];
+      const uint32_t p = prod[i];
+      b = num_bin_for(v[q], p, (uint64_t)hi[i] - lo[i] + 1, pol);
+    }
+    bin_append(b, (uint32_t)i, ctr->num_count, num_bins, n);
+  }
+}
+
+// ---------------------------------------------------------------- murmur3
+// 32-bit MurmurHash3 of one 4-byte little-endian key (public-domain algorithm by
+// Austin Appleby; reference: kernels/MurmurHash.cuh:44-98).
+__device__ __forceinline__ uint32_t murmur3_u32(uint32_t key, uint32_t seed) {
+  uint32_t k = key * 0xcc9e2d51u;
+  k = (k << 15) | (k >> 17);
+  k *= 0x1b873593u;
+  uint32_t h = seed ^ k;
+  h = (h << 13) | (h >> 19);
+  h = h * 5u + 0xe6546b64u;
+  h ^= 4u;
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+__global__ void k_murmur3(const uint32_t* __restrict__ keys, uint32_t* __restrict__ out, uint64_t n,
+                          uint32_t seed) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = murmur3_u32(keys[i], seed);
+}
+
+// ---------------------------------------------------------------- launchers
+namespace {
+constexpr size_t kNumBitmapSmem = sizeof(BitmapNumSmem);
+constexpr size_t kSymBitmapSmem = sizeof(unsigned long long) * kBitmapWords;
+template <int LOG2T>
+constexpr size_t num_hash_smem() { return (size_t)(1 << LOG2T) * 12; }
+template <int LOG2T>
+constexpr size_t sym_hash_smem() { return (size_t)(1 << LOG2T) * 4; }
+
+int g_occ[16];  // resident blocks per SM of each persistent kernel (same order as kinds)
+enum Kind { K_SYM_ESC, K_SYM_S, K_SYM_M, K_SYM_L, K_SYM_BM, K_NUM_ESC, K_NUM_S, K_NUM_M, K_NUM_L, K_NUM_BM };
+
+template <typename F>
+int occ_of(F f, int threads, size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, threads, smem) != cudaSuccess || n < 1) n = 1;
+  return n;
+}
+
+template <typename RP>
+void set_attrs() {
+  cudaFuncSetAttribute(k_sym_bitmap<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSymBitmapSmem);
+  cudaFuncSetAttribute(k_num_bitmap<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNumBitmapSmem);
+  cudaFuncSetAttribute(k_sym_hash<RP, 512, 15>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sym_hash_smem<15>());
+  cudaFuncSetAttribute(k_sym_hash<RP, 256, 13>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sym_hash_smem<13>());
+  cudaFuncSetAttribute(k_num_hash<RP, 512, 13>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)num_hash_smem<13>());
+  cudaFuncSetAttribute(k_num_hash<RP, 256, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)num_hash_smem<12>());
+}
+}  // namespace
+
+void configure_kernel_attributes() {
+  set_attrs<uint32_t>();
+  set_attrs<uint64_t>();
+  g_occ[K_SYM_ESC] = occ_of(k_sym_esc<uint32_t>, 256, 0);
+  g_occ[K_SYM_S] = occ_of(k_sym_hash<uint32_t, 128, 11>, 128, sym_hash_smem<11>());
+  g_occ[K_SYM_M] = occ_of(k_sym_hash<uint32_t, 256, 13>, 256, sym_hash_smem<13>());
+  g_occ[K_SYM_L] = occ_of(k_sym_hash<uint32_t, 512, 15>, 512, sym_hash_smem<15>());
+  g_occ[K_SYM_BM] = occ_of(k_sym_bitmap<uint32_t>, kBitmapThreads, kSymBitmapSmem);
+  g_occ[K_NUM_ESC] = occ_of(k_num_esc<uint32_t>, 256, 0);
+  g_occ[K_NUM_S] = occ_of(k_num_hash<uint32_t, 128, 10>, 128, num_hash_smem<10>());
+  g_occ[K_NUM_M] = occ_of(k_num_hash<uint32_t, 256, 12>, 256, num_hash_smem<12>());
+  g_occ[K_NUM_L] = occ_of(k_num_hash<uint32_t, 512, 13>, 512, num_hash_smem<13>());
+  g_occ[K_NUM_BM] = occ_of(k_num_bitmap<uint32_t>, kBitmapThreads, kNumBitmapSmem);
+}
+
+template <typename RP>
+void launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
+                     cudaStream_t s) {
+  if (A.rows == 0) return;
+  const double avg = (double)A.nnz / (double)A.rows;
+  if (avg >= 12.0) {
+    const uint64_t threads = A.rows * 32;
+    k_analysis<RP, 32><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
+        A, B, w.prod, w.lo, w.hi, w.row_nnz, w.sym_bins, w.ctr, pol);
+  } else {
+    const uint64_t threads = A.rows * 4;
+    k_analysis<RP, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
+        A, B, w.prod, w.lo, w.hi, w.row_nnz, w.sym_bins, w.ctr, pol);
+  }
+}
+
+template <typename RP>
+void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms, cudaStream_t s) {
+  if (A.rows == 0) return;
+  k_sym_esc<RP><<<num_sms * g_occ[K_SYM_ESC], 256, 0, s>>>(A, B, w.sym_bins, w.ctr, w.row_nnz);
+  k_sym_hash<RP, 128, 11><<<num_sms * g_occ[K_SYM_S], 128, sym_hash_smem<11>(), s>>>(
+      A, B, w.sym_bins, w.ctr, SB_HASH_S, w.prod, w.row_nnz);
+  k_sym_hash<RP, 256, 13><<<num_sms * g_occ[K_SYM_M], 256, sym_hash_smem<13>(), s>>>(
+      A, B, w.sym_bins, w.ctr, SB_HASH_M, w.prod, w.row_nnz);
+  k_sym_hash<RP, 512, 15><<<num_sms * g_occ[K_SYM_L], 512, sym_hash_smem<15>(), s>>>(
+      A, B, w.sym_bins, w.ctr, SB_HASH_L, w.prod, w.row_nnz);
+  k_sym_bitmap<RP><<<num_sms * g_occ[K_SYM_BM], kBitmapThreads, kSymBitmapSmem, s>>>(
+      A, B, w.sym_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz);
+}
+
+void launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s) {
+  const uint64_t nt = scan_tiles(w.rows);
+  if (w.rows == 0) return;
+  k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums);
+  k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, w.ctr, w.rowptr64, w.rowptr32, w.rows);
+  k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums, w.rowptr64, w.rowptr32,
+                                             w.prod, w.lo, w.hi, w.num_bins, w.ctr, pol);
+}
+
+template <typename RP>
+void launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_t* c_col, double* c_val,
+                    int num_sms, cudaStream_t s, cudaEvent_t* ev) {
+  if (A.rows == 0) return;
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ev[i], s);
+  };
+  mark(0);
+  k_num_esc<RP><<<num_sms * g_occ[K_NUM_ESC], 256, 0, s>>>(A, B, w.num_bins, w.ctr, w.row_nnz,
+                                                            w.rowptr64, c_col, c_val);
+  mark(1);
+  k_num_hash<RP, 128, 10><<<num_sms * g_occ[K_NUM_S], 128, num_hash_smem<10>(), s>>>(
+      A, B, w.num_bins, w.ctr, NB_HASH_S, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(2);
+  k_num_hash<RP, 256, 12><<<num_sms * g_occ[K_NUM_M], 256, num_hash_smem<12>(), s>>>(
+      A, B, w.num_bins, w.ctr, NB_HASH_M, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(3);
+  k_num_hash<RP, 512, 13><<<num_sms * g_occ[K_NUM_L], 512, num_hash_smem<13>(), s>>>(
+      A, B, w.num_bins, w.ctr, NB_HASH_L, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(4);
+  k_num_bitmap<RP><<<num_sms * g_occ[K_NUM_BM], kBitmapThreads, kNumBitmapSmem, s>>>(
+      A, B, w.num_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(5);
+}
+
+void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, cudaStream_t s) {
+  if (n == 0) return;
+  const uint64_t blocks = (n + 255) / 256;
+  k_murmur3<<<(unsigned)(blocks > 4096 ? 4096 : blocks), 256, 0, s>>>(keys, out, n, seed);
+}
+
+template void launch_analysis<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
+                                        const SymPolicy&, cudaStream_t);
+template void launch_analysis<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
+                                        const SymPolicy&, cudaStream_t);
+template void launch_symbolic<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, int,
+                                        cudaStream_t);
+template void launch_symbolic<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, int,
+                                        cudaStream_t);
+template void launch_numeric<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
+                                       uint32_t*, double*, int, cudaStream_t, cudaEvent_t*);
+template void launch_numeric<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
+                                       uint32_t*, double*, int, cudaStream_t, cudaEvent_t*);
+
+}  // namespace ocean

@@ -1,0 +1,645 @@
+// C ABI and host orchestration of one SpGEMM (C = A·B).
+//
+// Replaces somespgemm::SpGEMM::run (kernels/SpGEMM.cuh:213-338). The reference
+// runs one of four workflows with ~18 blocking read-backs and 20 streams; this
+// orchestration runs analysis -> symbolic -> scan -> (one read-back of nnz(C)
+// to allocate C) -> numeric, with every row class handled by a persistent
+// kernel that reads its row list and count from device memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "config.h"
+#include "kernels.h"
+#include "ocean.h"
+
+using namespace ocean;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct OceanError {
+  int code;
+  std::string msg;
+};
+
+#define OCEAN_CUDA(call)                                                                          \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) {                                                                      \
+      throw OceanError{e_ == cudaErrorMemoryAllocation ? (int)OCEAN_ERR_OOM : (int)OCEAN_ERR_CUDA, \
+                       std::string(#call) + ": " + cudaGetErrorString(e_)};                       \
+    }                                                                                             \
+  } while (0)
+
+#define OCEAN_CHECK(cond, code, msg)        \
+  do {                                      \
+    if (!(cond)) throw OceanError{code, msg}; \
+  } while (0)
+
+// Allocation record of a result (C->_owner).
+struct CResult {
+  int location;  // 0 device (owned), 1 host (lent by the handle)
+  void* rowptr = nullptr;
+  uint32_t* col = nullptr;
+  double* val = nullptr;
+};
+
+enum Ev {
+  EV_START = 0,
+  EV_ANALYSIS,
+  EV_SYMBOLIC,
+  EV_SCAN,
+  EV_NUM0,  // EV_NUM0 .. EV_NUM0+5: numeric class boundaries
+  EV_NUM_END = EV_NUM0 + 5,
+  EV_END,
+  EV_COUNT
+};
+
+struct Stats {
+  uint64_t a_rows = 0, a_cols = 0, a_nnz = 0, b_rows = 0, b_cols = 0, b_nnz = 0;
+  uint64_t c_rows = 0, c_cols = 0, c_nnz = 0;
+  uint64_t total_products = 0;
+  uint32_t max_products = 0, max_a_nnz = 0;
+  uint32_t sym_bins[SB_COUNT] = {0};
+  uint32_t num_bins[NB_COUNT] = {0};
+  int workflow = 0;  // 0 = precise (symbolic + numeric)
+  int rowptr_bits = 32;
+  bool valid = false;
+  double host_ms = 0.0;
+};
+
+__global__ void k_widen_rowptr(const uint32_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
+template <typename T>
+void grow(T*& p, uint64_t& cap, uint64_t need) {
+  if (need <= cap && p) return;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  const uint64_t n = std::max<uint64_t>(need, 1);
+  OCEAN_CUDA(cudaMalloc((void**)&p, n * sizeof(T)));
+  cap = n;
+}
+
+template <typename T>
+void grow_host(T*& p, uint64_t& cap, uint64_t need) {
+  if (need <= cap && p) return;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  cap = 0;
+  const uint64_t n = std::max<uint64_t>(need, 1);
+  OCEAN_CUDA(cudaHostAlloc((void**)&p, n * sizeof(T), cudaHostAllocDefault));
+  cap = n;
+}
+
+}  // namespace
+
+struct ocean_handle {
+  Config cfg;
+  int device = 0;
+  int num_sms = 148;
+  DevWork w;
+  uint64_t cap_rows = 0;
+  DevCounters* h_ctr = nullptr;  // pinned
+  cudaEvent_t ev[EV_COUNT];
+  bool ev_recorded = false;
+  bool tracked = false;
+  Stats st;
+  // widened row pointers for mixed 32/64-bit inputs
+  uint64_t* wide_a = nullptr;
+  uint64_t wide_a_cap = 0;
+  uint64_t* wide_b = nullptr;
+  uint64_t wide_b_cap = 0;
+  // device copies of host inputs (ocean_spgemm_host)
+  unsigned char* in_rp[2] = {nullptr, nullptr};
+  uint64_t in_rp_cap[2] = {0, 0};
+  uint32_t* in_col[2] = {nullptr, nullptr};
+  uint64_t in_col_cap[2] = {0, 0};
+  double* in_val[2] = {nullptr, nullptr};
+  uint64_t in_val_cap[2] = {0, 0};
+  // pinned host output (ocean_spgemm_host)
+  unsigned char* out_rp = nullptr;
+  uint64_t out_rp_cap = 0;
+  uint32_t* out_col = nullptr;
+  uint64_t out_col_cap = 0;
+  double* out_val = nullptr;
+  uint64_t out_val_cap = 0;
+  CResult host_owner{1};
+
+  void free_all() {
+    DevWork& x = w;
+    void* ps[] = {x.prod, x.lo, x.hi, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32,
+                  x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
+    for (void* p : ps)
+      if (p) cudaFree(p);
+    if (h_ctr) cudaFreeHost(h_ctr);
+    if (out_rp) cudaFreeHost(out_rp);
+    if (out_col) cudaFreeHost(out_col);
+    if (out_val) cudaFreeHost(out_val);
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+};
+
+namespace {
+
+void init_handle(ocean_handle* h, const std::string& json) {
+  h->cfg = Config::from_json_text(json);
+  OCEAN_CUDA(cudaGetDevice(&h->device));
+  OCEAN_CUDA(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+  // Stream-ordered allocations come from the device's default pool, which is told
+  // to keep freed memory (as the reference does, kernels/SpGEMM.cuh:219-223).
+  cudaMemPool_t pool;
+  OCEAN_CUDA(cudaDeviceGetDefaultMemPool(&pool, h->device));
+  uint64_t threshold = UINT64_MAX;
+  OCEAN_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+  static bool configured[64] = {false};
+  if (h->device < 64 && !configured[h->device]) {
+    configure_kernel_attributes();
+    OCEAN_CUDA(cudaGetLastError());
+    configured[h->device] = true;
+  }
+  for (auto& e : h->ev) OCEAN_CUDA(cudaEventCreate(&e));
+  OCEAN_CUDA(cudaHostAlloc((void**)&h->h_ctr, sizeof(DevCounters), cudaHostAllocDefault));
+  OCEAN_CUDA(cudaMalloc((void**)&h->w.ctr, sizeof(DevCounters)));
+}
+
+void ensure_rows(ocean_handle* h, uint64_t rows) {
+  if (rows <= h->cap_rows && h->w.prod) {
+    h->w.rows = rows;
+    return;
+  }
+  DevWork& x = h->w;
+  void* ps[] = {x.prod, x.lo, x.hi, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  const uint64_t r = std::max<uint64_t>(rows, 1);
+  OCEAN_CUDA(cudaMalloc((void**)&x.prod, r * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.lo, r * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.hi, r * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.row_nnz, r * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.sym_bins, r * 4 * SB_COUNT));
+  OCEAN_CUDA(cudaMalloc((void**)&x.num_bins, r * 4 * NB_COUNT));
+  OCEAN_CUDA(cudaMalloc((void**)&x.tile_sums, scan_tiles(r) * 8 + 8));
+  OCEAN_CUDA(cudaMalloc((void**)&x.rowptr64, (r + 1) * 8));
+  OCEAN_CUDA(cudaMalloc((void**)&x.rowptr32, (r + 1) * 4));
+  h->cap_rows = r;
+  x.rows = rows;
+}
+
+void validate_view(const ocean_csr_view* m, const char* name) {
+  OCEAN_CHECK(m != nullptr, OCEAN_ERR_INVALID, std::string(name) + " is NULL");
+  OCEAN_CHECK(m->rowptr_bits == 32 || m->rowptr_bits == 64, OCEAN_ERR_INVALID,
+              std::string(name) + ".rowptr_bits must be 32 or 64");
+  OCEAN_CHECK(m->rows == 0 || m->rowptr != nullptr, OCEAN_ERR_INVALID, std::string(name) + ".rowptr is NULL");
+  OCEAN_CHECK(m->nnz == 0 || (m->col != nullptr && m->val != nullptr), OCEAN_ERR_INVALID,
+              std::string(name) + ".col/.val is NULL");
+  OCEAN_CHECK(m->rows < 0xFFFFFFFFull, OCEAN_ERR_INVALID, std::string(name) + " has too many rows (>= 2^32-1)");
+  OCEAN_CHECK(m->cols <= 0xFFFFFFFFull, OCEAN_ERR_INVALID, std::string(name) + " has too many columns (> 2^32-1)");
+  OCEAN_CHECK(m->rowptr_bits == 64 || m->nnz <= 0xFFFFFFFFull, OCEAN_ERR_INVALID,
+              std::string(name) + " has nnz >= 2^32 with 32-bit row pointers");
+}
+
+void record(ocean_handle* h, int i, cudaStream_t s) { cudaEventRecord(h->ev[i], s); }
+
+const char* status_text(unsigned st) {
+  if (st & DEV_TABLE_FULL) return "a shared-memory hash table ran full (probe limit reached)";
+  if (st & DEV_BIN_OVERFLOW) return "a row exceeded the capacity of its accumulator class";
+  if (st & DEV_COUNT_MISMATCH) return "numeric output count differs from the symbolic count";
+  return "device error";
+}
+
+void check_device_status(ocean_handle* h) {
+  if (h->h_ctr->status) {
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s (status 0x%x, first row %u)", status_text(h->h_ctr->status), h->h_ctr->status,
+             h->h_ctr->err_row);
+    throw OceanError{(h->h_ctr->status & DEV_COUNT_MISMATCH) ? (int)OCEAN_ERR_INTERNAL : (int)OCEAN_ERR_CAPACITY,
+                     buf};
+  }
+}
+
+template <typename RP>
+Csr<RP> to_csr(const ocean_csr_view* m, const RP* rp) {
+  Csr<RP> c;
+  c.rows = m->rows;
+  c.cols = m->cols;
+  c.nnz = m->nnz;
+  c.rp = rp;
+  c.col = m->col;
+  c.val = m->val;
+  return c;
+}
+
+// Runs analysis + symbolic + scan. Leaves exact per-row counts in w.row_nnz,
+// row pointers in w.rowptr64/32 and the counters in h->h_ctr (read back).
+template <typename RP>
+void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool with_scan) {
+  ensure_rows(h, A.rows);
+  OCEAN_CUDA(cudaMemsetAsync(h->w.ctr, 0, sizeof(DevCounters), s));
+  SymPolicy sp;
+  sp.esc_max_products = (uint32_t)h->cfg.esc_max_products;
+  sp.force_bin = h->cfg.force_sym_bin;
+  NumPolicy np;
+  np.esc_max_products = (uint32_t)h->cfg.esc_max_products;
+  np.force_bin = h->cfg.force_num_bin;
+  OCEAN_CHECK(sp.force_bin < SB_COUNT && np.force_bin < NB_COUNT, OCEAN_ERR_INVALID, "forced class out of range");
+  record(h, EV_START, s);
+  launch_analysis(A, B, h->w, sp, s);
+  OCEAN_CUDA(cudaGetLastError());
+  record(h, EV_ANALYSIS, s);
+  launch_symbolic(A, B, h->w, h->num_sms, s);
+  OCEAN_CUDA(cudaGetLastError());
+  record(h, EV_SYMBOLIC, s);
+  if (with_scan) {
+    launch_scan(h->w, np, s);
+    OCEAN_CUDA(cudaGetLastError());
+  }
+  record(h, EV_SCAN, s);
+  OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+  OCEAN_CUDA(cudaStreamSynchronize(s));
+  check_device_status(h);
+}
+
+template <typename RP>
+void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view* Bv, const RP* arp,
+                const RP* brp, ocean_csr* C, cudaStream_t s) {
+  const auto t0 = std::chrono::steady_clock::now();
+  const Csr<RP> A = to_csr<RP>(Av, arp);
+  const Csr<RP> B = to_csr<RP>(Bv, brp);
+  Stats& st = h->st;
+  st = Stats();
+  st.a_rows = A.rows, st.a_cols = A.cols, st.a_nnz = A.nnz;
+  st.b_rows = B.rows, st.b_cols = B.cols, st.b_nnz = B.nnz;
+  h->ev_recorded = false;
+
+  uint64_t nnz = 0;
+  if (A.rows > 0) {
+    run_front(h, A, B, s, true);
+    nnz = h->h_ctr->total_nnz;
+  } else {
+    std::memset(h->h_ctr, 0, sizeof(DevCounters));
+  }
+  int bits = h->cfg.output_rowptr_bits ? h->cfg.output_rowptr_bits : (nnz >= (1ull << 32) ? 64 : 32);
+  OCEAN_CHECK(!(bits == 32 && nnz >= (1ull << 32)), OCEAN_ERR_INVALID,
+              "nnz(C) >= 2^32 does not fit 32-bit row pointers (output_rowptr_bits=32)");
+  CResult* owner = new CResult{0};
+  try {
+    OCEAN_CUDA(cudaMallocAsync(&owner->rowptr, (A.rows + 1) * (bits / 8), s));
+    OCEAN_CUDA(cudaMallocAsync((void**)&owner->col, std::max<uint64_t>(nnz, 1) * 4, s));
+    OCEAN_CUDA(cudaMallocAsync((void**)&owner->val, std::max<uint64_t>(nnz, 1) * 8, s));
+    if (A.rows > 0) {
+      launch_numeric(A, B, h->w, owner->col, owner->val, h->num_sms, s, h->ev + EV_NUM0);
+      OCEAN_CUDA(cudaGetLastError());
+      OCEAN_CUDA(cudaMemcpyAsync(owner->rowptr, bits == 64 ? (void*)h->w.rowptr64 : (void*)h->w.rowptr32,
+                                 (A.rows + 1) * (bits / 8), cudaMemcpyDeviceToDevice, s));
+    } else {
+      OCEAN_CUDA(cudaMemsetAsync(owner->rowptr, 0, bits / 8, s));
+      for (int i = EV_START; i < EV_END; ++i) record(h, i, s);
+    }
+    record(h, EV_END, s);
+    h->ev_recorded = true;
+    h->tracked = h->cfg.track_stage_times;
+    if (h->cfg.sync_on_return && A.rows > 0) {
+      OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+      OCEAN_CUDA(cudaStreamSynchronize(s));
+      check_device_status(h);
+    }
+  } catch (...) {
+    if (owner->rowptr) cudaFreeAsync(owner->rowptr, s);
+    if (owner->col) cudaFreeAsync(owner->col, s);
+    if (owner->val) cudaFreeAsync(owner->val, s);
+    delete owner;
+    throw;
+  }
+  C->rows = A.rows;
+  C->cols = B.cols;
+  C->nnz = nnz;
+  C->rowptr = owner->rowptr;
+  C->rowptr_bits = bits;
+  C->col = owner->col;
+  C->val = owner->val;
+  C->location = 0;
+  C->_owner = owner;
+
+  st.c_rows = A.rows, st.c_cols = B.cols, st.c_nnz = nnz;
+  st.total_products = h->h_ctr->total_products;
+  st.max_products = h->h_ctr->max_products;
+  st.max_a_nnz = h->h_ctr->max_a_nnz;
+  for (int i = 0; i < SB_COUNT; ++i) st.sym_bins[i] = h->h_ctr->sym_count[i];
+  for (int i = 0; i < NB_COUNT; ++i) st.num_bins[i] = h->h_ctr->num_count[i];
+  st.rowptr_bits = bits;
+  st.workflow = 0;
+  st.valid = true;
+  st.host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Dispatch on row-pointer widths (mixed widths are widened to 64 bits).
+void dispatch_spgemm(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, ocean_csr* C,
+                     cudaStream_t s) {
+  validate_view(A, "A");
+  validate_view(B, "B");
+  OCEAN_CHECK(A->cols == B->rows, OCEAN_ERR_INVALID, "Incompatible matrix dimensions (A.cols != B.rows)");
+  OCEAN_CHECK(C != nullptr, OCEAN_ERR_INVALID, "C is NULL");
+  OCEAN_CHECK(!(h->cfg.use_hybrid_accumulator && !h->cfg.use_indirect_sort), OCEAN_ERR_INVALID,
+              "Invalid configuration: use_hybrid_accumulator requires use_indirect_sort");
+  if (A->rowptr_bits == 32 && B->rowptr_bits == 32) {
+    run_spgemm<uint32_t>(h, A, B, (const uint32_t*)A->rowptr, (const uint32_t*)B->rowptr, C, s);
+    return;
+  }
+  const uint64_t* arp = (const uint64_t*)A->rowptr;
+  const uint64_t* brp = (const uint64_t*)B->rowptr;
+  if (A->rowptr_bits == 32 && A->rows) {
+    grow(h->wide_a, h->wide_a_cap, A->rows + 1);
+    k_widen_rowptr<<<256, 256, 0, s>>>((const uint32_t*)A->rowptr, h->wide_a, A->rows);
+    arp = h->wide_a;
+  }
+  if (B->rowptr_bits == 32 && B->rows) {
+    grow(h->wide_b, h->wide_b_cap, B->rows + 1);
+    k_widen_rowptr<<<256, 256, 0, s>>>((const uint32_t*)B->rowptr, h->wide_b, B->rows);
+    brp = h->wide_b;
+  }
+  OCEAN_CUDA(cudaGetLastError());
+  run_spgemm<uint64_t>(h, A, B, arp, brp, C, s);
+}
+
+double ev_ms(ocean_handle* h, int a, int b) {
+  if (!h->ev_recorded) return -1.0;
+  if (cudaEventSynchronize(h->ev[b]) != cudaSuccess) return -1.0;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[a], h->ev[b]) != cudaSuccess) return -1.0;
+  return ms;
+}
+
+std::string stats_json(ocean_handle* h) {
+  const Stats& st = h->st;
+  std::ostringstream o;
+  o.precision(17);
+  auto dims = [&](const char* n, uint64_t r, uint64_t c, uint64_t z) {
+    o << "\"" << n << "\": {\"rows\": " << r << ", \"cols\": " << c << ", \"nnz\": " << z << "}, ";
+  };
+  o << "{";
+  dims("A", st.a_rows, st.a_cols, st.a_nnz);
+  dims("B", st.b_rows, st.b_cols, st.b_nnz);
+  dims("C", st.c_rows, st.c_cols, st.c_nnz);
+  const double avg = st.a_rows ? (double)st.total_products / (double)st.a_rows : 0.0;
+  const double ie = st.a_nnz ? (double)st.total_products / (double)st.a_nnz : 0.0;
+  const double oc = st.c_nnz ? (double)st.total_products / (double)st.c_nnz : 0.0;
+  o << "\"stats\": {\"intermediate_product\": " << st.total_products
+    << ", \"intermediate_product_max\": " << st.max_products << ", \"intermediate_product_avg\": " << avg
+    << ", \"input_expansion\": " << ie << ", \"output_compression\": " << oc
+    << ", \"max_a_row_nnz\": " << st.max_a_nnz << "}, ";
+  o << "\"decision\": {\"workflow\": " << st.workflow << ", \"rowptr_bits\": " << st.rowptr_bits << "}, ";
+  o << "\"binning_1\": [";
+  for (int i = 0; i < SB_COUNT; ++i) o << (i ? ", " : "") << st.sym_bins[i];
+  o << "], \"binning_2\": [";
+  for (int i = 0; i < NB_COUNT; ++i) o << (i ? ", " : "") << st.num_bins[i];
+  o << "], ";
+  const double total = ev_ms(h, EV_START, EV_END);
+  if (h->tracked) {
+    o << "\"timing\": {\"analysis\": " << ev_ms(h, EV_START, EV_ANALYSIS)
+      << ", \"symbolic\": " << ev_ms(h, EV_ANALYSIS, EV_SYMBOLIC) << ", \"scan\": " << ev_ms(h, EV_SYMBOLIC, EV_SCAN)
+      << ", \"numeric\": " << ev_ms(h, EV_NUM0, EV_NUM_END) << ", \"numeric_esc\": " << ev_ms(h, EV_NUM0, EV_NUM0 + 1)
+      << ", \"numeric_hash_s\": " << ev_ms(h, EV_NUM0 + 1, EV_NUM0 + 2)
+      << ", \"numeric_hash_m\": " << ev_ms(h, EV_NUM0 + 2, EV_NUM0 + 3)
+      << ", \"numeric_hash_l\": " << ev_ms(h, EV_NUM0 + 3, EV_NUM0 + 4)
+      << ", \"numeric_bitmap\": " << ev_ms(h, EV_NUM0 + 4, EV_NUM0 + 5) << ", \"host_ms\": " << st.host_ms << "}, ";
+  }
+  o << "\"total_time\": " << total << ", \"gflops\": "
+    << (total > 0 ? 2.0 * (double)st.total_products / total / 1e6 : 0.0) << "}";
+  return o.str();
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return OCEAN_OK;
+  } catch (const OceanError& e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return OCEAN_ERR_INVALID;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return OCEAN_ERR_OOM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return OCEAN_ERR_INTERNAL;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ocean_create(ocean_handle** out, const char* json_config) {
+  return guarded([&] {
+    OCEAN_CHECK(out != nullptr, OCEAN_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    ocean_handle* h = new ocean_handle();
+    try {
+      init_handle(h, json_config ? std::string(json_config) : std::string());
+    } catch (...) {
+      h->free_all();
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int ocean_create_from_file(ocean_handle** out, const char* json_path) {
+  return guarded([&] {
+    OCEAN_CHECK(json_path != nullptr, OCEAN_ERR_INVALID, "json_path is NULL");
+    std::ifstream f(json_path);
+    OCEAN_CHECK(f.good(), OCEAN_ERR_INVALID, std::string("cannot open config file ") + json_path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string text = ss.str();
+    const int rc = ocean_create(out, text.c_str());
+    if (rc != OCEAN_OK) throw OceanError{rc, g_last_error};
+  });
+}
+
+void ocean_destroy(ocean_handle* h) {
+  if (!h) return;
+  h->free_all();
+  delete h;
+}
+
+int ocean_spgemm(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, ocean_csr* C, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    dispatch_spgemm(h, A, B, C, (cudaStream_t)stream);
+  });
+}
+
+int ocean_spgemm_host(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, ocean_csr* C,
+                      void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    validate_view(A, "A");
+    validate_view(B, "B");
+    OCEAN_CHECK(C != nullptr, OCEAN_ERR_INVALID, "C is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    ocean_csr_view dv[2];
+    const ocean_csr_view* src[2] = {A, B};
+    const bool same = A->rowptr == B->rowptr && A->col == B->col && A->val == B->val && A->rows == B->rows &&
+                      A->nnz == B->nnz && A->rowptr_bits == B->rowptr_bits;
+    for (int m = 0; m < (same ? 1 : 2); ++m) {
+      const ocean_csr_view* v = src[m];
+      const uint64_t rpb = (v->rows + 1) * (uint64_t)(v->rowptr_bits / 8);
+      grow(h->in_rp[m], h->in_rp_cap[m], rpb);
+      grow(h->in_col[m], h->in_col_cap[m], v->nnz);
+      grow(h->in_val[m], h->in_val_cap[m], v->nnz);
+      if (v->rows) OCEAN_CUDA(cudaMemcpyAsync(h->in_rp[m], v->rowptr, rpb, cudaMemcpyHostToDevice, s));
+      if (v->nnz) {
+        OCEAN_CUDA(cudaMemcpyAsync(h->in_col[m], v->col, v->nnz * 4, cudaMemcpyHostToDevice, s));
+        OCEAN_CUDA(cudaMemcpyAsync(h->in_val[m], v->val, v->nnz * 8, cudaMemcpyHostToDevice, s));
+      }
+      dv[m] = *v;
+      dv[m].rowptr = h->in_rp[m];
+      dv[m].col = h->in_col[m];
+      dv[m].val = h->in_val[m];
+    }
+    if (same) dv[1] = dv[0];
+    ocean_csr dc;
+    dispatch_spgemm(h, &dv[0], &dv[1], &dc, s);
+    const uint64_t rpb = (dc.rows + 1) * (uint64_t)(dc.rowptr_bits / 8);
+    CResult* dev_owner = (CResult*)dc._owner;
+    try {
+      grow_host(h->out_rp, h->out_rp_cap, rpb);
+      grow_host(h->out_col, h->out_col_cap, dc.nnz);
+      grow_host(h->out_val, h->out_val_cap, dc.nnz);
+      OCEAN_CUDA(cudaMemcpyAsync(h->out_rp, dc.rowptr, rpb, cudaMemcpyDeviceToHost, s));
+      if (dc.nnz) {
+        OCEAN_CUDA(cudaMemcpyAsync(h->out_col, dc.col, dc.nnz * 4, cudaMemcpyDeviceToHost, s));
+        OCEAN_CUDA(cudaMemcpyAsync(h->out_val, dc.val, dc.nnz * 8, cudaMemcpyDeviceToHost, s));
+      }
+    } catch (...) {
+      cudaFreeAsync(dev_owner->rowptr, s);
+      cudaFreeAsync(dev_owner->col, s);
+      cudaFreeAsync(dev_owner->val, s);
+      delete dev_owner;
+      throw;
+    }
+    OCEAN_CUDA(cudaFreeAsync(dev_owner->rowptr, s));
+    OCEAN_CUDA(cudaFreeAsync(dev_owner->col, s));
+    OCEAN_CUDA(cudaFreeAsync(dev_owner->val, s));
+    delete dev_owner;
+    OCEAN_CUDA(cudaStreamSynchronize(s));
+    *C = dc;
+    C->rowptr = h->out_rp;
+    C->col = h->out_col;
+    C->val = h->out_val;
+    C->location = 1;
+    C->_owner = &h->host_owner;
+  });
+}
+
+int ocean_csr_free(ocean_csr* C, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(C != nullptr, OCEAN_ERR_INVALID, "C is NULL");
+    CResult* o = (CResult*)C->_owner;
+    if (o && o->location == 0) {
+      cudaStream_t s = (cudaStream_t)stream;
+      OCEAN_CUDA(cudaFreeAsync(o->rowptr, s));
+      OCEAN_CUDA(cudaFreeAsync(o->col, s));
+      OCEAN_CUDA(cudaFreeAsync(o->val, s));
+      delete o;
+    }
+    std::memset(C, 0, sizeof(*C));
+  });
+}
+
+int ocean_csr_download(const ocean_csr* C, void* rowptr, uint32_t* col, double* val, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(C != nullptr, OCEAN_ERR_INVALID, "C is NULL");
+    OCEAN_CHECK(rowptr != nullptr && (C->nnz == 0 || (col && val)), OCEAN_ERR_INVALID, "output buffer is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    const cudaMemcpyKind kind = C->location == 1 ? cudaMemcpyHostToHost : cudaMemcpyDeviceToHost;
+    OCEAN_CUDA(cudaMemcpyAsync(rowptr, C->rowptr, (C->rows + 1) * (uint64_t)(C->rowptr_bits / 8), kind, s));
+    if (C->nnz) {
+      OCEAN_CUDA(cudaMemcpyAsync(col, C->col, C->nnz * 4, kind, s));
+      OCEAN_CUDA(cudaMemcpyAsync(val, C->val, C->nnz * 8, kind, s));
+    }
+    OCEAN_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int ocean_symbolic(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, uint32_t* row_nnz,
+                   void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    validate_view(A, "A");
+    validate_view(B, "B");
+    OCEAN_CHECK(A->cols == B->rows, OCEAN_ERR_INVALID, "Incompatible matrix dimensions (A.cols != B.rows)");
+    OCEAN_CHECK(A->rows == 0 || row_nnz != nullptr, OCEAN_ERR_INVALID, "row_nnz is NULL");
+    OCEAN_CHECK(A->rowptr_bits == B->rowptr_bits, OCEAN_ERR_INVALID,
+                "ocean_symbolic needs equal row-pointer widths for A and B");
+    if (A->rows == 0) return;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (A->rowptr_bits == 32) {
+      run_front(h, to_csr<uint32_t>(A, (const uint32_t*)A->rowptr), to_csr<uint32_t>(B, (const uint32_t*)B->rowptr),
+                s, false);
+    } else {
+      run_front(h, to_csr<uint64_t>(A, (const uint64_t*)A->rowptr), to_csr<uint64_t>(B, (const uint64_t*)B->rowptr),
+                s, false);
+    }
+    OCEAN_CUDA(cudaMemcpyAsync(row_nnz, h->w.row_nnz, A->rows * 4, cudaMemcpyDeviceToDevice, s));
+    OCEAN_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int ocean_stats_json(ocean_handle* h, char* buf, size_t cap, size_t* needed) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    const std::string js = stats_json(h);
+    if (needed) *needed = js.size() + 1;
+    OCEAN_CHECK(buf == nullptr || cap >= js.size() + 1, OCEAN_ERR_CAPACITY, "stats buffer too small");
+    if (buf) std::memcpy(buf, js.c_str(), js.size() + 1);
+  });
+}
+
+double ocean_stage_ms(ocean_handle* h, const char* stage) {
+  if (!h || !stage || !h->ev_recorded) return -1.0;
+  const std::string s(stage);
+  if (s == "total") return ev_ms(h, EV_START, EV_END);
+  if (!h->tracked) return -1.0;
+  if (s == "analysis") return ev_ms(h, EV_START, EV_ANALYSIS);
+  if (s == "symbolic") return ev_ms(h, EV_ANALYSIS, EV_SYMBOLIC);
+  if (s == "scan") return ev_ms(h, EV_SYMBOLIC, EV_SCAN);
+  if (s == "numeric") return ev_ms(h, EV_NUM0, EV_NUM_END);
+  if (s == "numeric_esc") return ev_ms(h, EV_NUM0, EV_NUM0 + 1);
+  if (s == "numeric_hash_s") return ev_ms(h, EV_NUM0 + 1, EV_NUM0 + 2);
+  if (s == "numeric_hash_m") return ev_ms(h, EV_NUM0 + 2, EV_NUM0 + 3);
+  if (s == "numeric_hash_l") return ev_ms(h, EV_NUM0 + 3, EV_NUM0 + 4);
+  if (s == "numeric_bitmap") return ev_ms(h, EV_NUM0 + 4, EV_NUM0 + 5);
+  return -1.0;
+}
+
+int ocean_murmur3_u32(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(n == 0 || (keys && out), OCEAN_ERR_INVALID, "keys/out is NULL");
+    launch_murmur3(keys, out, n, seed, (cudaStream_t)stream);
+    OCEAN_CUDA(cudaGetLastError());
+  });
+}
+
+const char* ocean_last_error(void) { return g_last_error.c_str(); }
+const char* ocean_version(void) { return "ocean-b200 0.1.0"; }
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+// Internal types and device helpers shared by the SpGEMM kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ocean {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// Bitmap accumulator window: 2^20 columns per pass (128 KB of bits in shared
+// memory). A row whose output column span is wider is swept in several windows.
+constexpr int kBitmapLog2 = 20;
+constexpr uint64_t kBitmapBits = 1ull << kBitmapLog2;
+constexpr int kBitmapWords = 1 << (kBitmapLog2 - 6);   // 64-bit words
+constexpr int kBitmapThreads = 1024;
+constexpr int kWordsPerThread = kBitmapWords / kBitmapThreads;  // 16
+constexpr int kSuperWords = 1024;                       // words per rank superblock
+constexpr int kSupers = kBitmapWords / kSuperWords;     // 16
+
+// Row classes ("bins"). Symbolic classes are chosen from the product count and
+// the column span, numeric classes from the exact output count.
+enum SymBin : int {
+  SB_ESC = 0,      // <= 32 products: one warp, match-any distinct count
+  SB_HASH_S = 1,   // hash set, 128 threads, 2048 slots
+  SB_HASH_M = 2,   // hash set, 256 threads, 8192 slots
+  SB_HASH_L = 3,   // hash set, 512 threads, 32768 slots
+  SB_BITMAP = 4,   // bitmap over the column span, 1024 threads
+  SB_COUNT = 5
+};
+enum NumBin : int {
+  NB_ESC = 0,      // <= 32 products: one warp, register sort + segmented sum
+  NB_HASH_S = 1,   // hash accumulate + sort, 128 threads, 1024 slots (<= 512 out)
+  NB_HASH_M = 2,   // 256 threads, 4096 slots (<= 2048 out)
+  NB_HASH_L = 3,   // 512 threads, 8192 slots (<= 4096 out)
+  NB_BITMAP = 4,   // bitmap-rank accumulator, any size
+  NB_COUNT = 5
+};
+
+// Device-side counters of one multiply (zeroed at the start of each call).
+struct DevCounters {
+  unsigned long long total_products;
+  unsigned long long total_nnz;
+  unsigned int max_products;
+  unsigned int max_a_nnz;
+  unsigned int sym_count[SB_COUNT];
+  unsigned int sym_cursor[SB_COUNT];
+  unsigned int num_count[NB_COUNT];
+  unsigned int num_cursor[NB_COUNT];
+  unsigned int status;     // OR of DevError bits
+  unsigned int err_row;
+  unsigned int pad[4];
+};
+
+enum DevError : unsigned int {
+  DEV_TABLE_FULL = 1u,     // an open-addressing probe exceeded the table size
+  DEV_BIN_OVERFLOW = 2u,   // a row did not fit the class it was placed in
+  DEV_COUNT_MISMATCH = 4u  // numeric output count differs from the symbolic count
+};
+
+// CSR view used by kernels. RP is the row-pointer type (uint32_t or uint64_t).
+template <typename RP>
+struct Csr {
+  uint64_t rows, cols, nnz;
+  const RP* rp;
+  const uint32_t* col;
+  const double* val;
+  __device__ __forceinline__ uint64_t row_begin(uint64_t r) const { return (uint64_t)rp[r]; }
+  __device__ __forceinline__ uint64_t row_end(uint64_t r) const {
+    return (r + 1 == rows) ? nnz : (uint64_t)rp[r + 1];
+  }
+};
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Warp-aggregated append of `row` to bin `b` (b < 0: no append).
+__device__ __forceinline__ void bin_append(int b, uint32_t row, unsigned int* counts,
+                                           uint32_t* bins, uint64_t stride) {
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(kFull, b);
+  const int leader = __ffs(peers) - 1;
+  unsigned base = 0;
+  if (lane == leader && b >= 0) base = atomicAdd(&counts[b], (unsigned)__popc(peers));
+  base = __shfl_sync(kFull, base, leader);
+  if (b >= 0) bins[(uint64_t)b * stride + base + __popc(peers & lanemask_lt())] = row;
+}
+
+// Group size (lanes per A element) for a row: enough lanes to cover the mean
+// B-row length, a power of two in [1, 32].
+__device__ __forceinline__ int group_size_for(uint64_t products, uint64_t a_nnz) {
+  if (a_nnz == 0) return 32;
+  const uint64_t avg = (products + a_nnz - 1) / a_nnz;
+  int g = 1;
+  while (g < 32 && (uint64_t)g < avg) g <<= 1;
+  return g;
+}
+
+// Multiplicative hash of a column id into [0, 2^log2).
+__device__ __forceinline__ uint32_t hash_slot(uint32_t c, int log2) {
+  return (c * 0x9E3779B1u) >> (32 - log2);
+}
+
+}  // namespace ocean
