@@ -1,0 +1,477 @@
+#!/usr/bin/env python
+"""SpGEMM benchmark: GFLOP/s (2 x intermediate products / s) of C = A·A on one B200.
+
+Workload (default "rmat20"): A = square R-MAT, n = 2^20, 16 edges per vertex,
+quadrant probabilities (0.57, 0.19, 0.19, 0.05), duplicate edges merged, FP64
+values uniform in [-1, 1], seed 0 (synthetic, seeded; no dataset download).
+C = A·A has ~2.1e10 intermediate products and ~9.7e9 entries (> 2^32, so C
+carries 64-bit row pointers; ~116 GB in HBM).
+
+One JSON line is printed by rank 0 with:
+  value      device-timed throughput, inputs resident in HBM (CUDA events on the
+             launching stream around K full multiplies, max over ranks);
+  e2e        the same metric through the host-buffer C ABI call
+             (ocean_spgemm_host): pinned host A in, C back in host memory, all
+             copies inside the timed region;
+  roofline   the dominant kernel's algorithmic bytes per launch / its
+             event-timed duration against the measured HBM copy bandwidth;
+  cpu_baseline  the CPU oracle (OpenMP Gustavson, all host cores) on a bounded
+             sample of the same rows.
+`--impl reference` times the CPU restatement of the path (the reference has no
+CPU SpGEMM; its GPU code is the comparison the library replaces) on bounded
+samples of the same workload and prints the same line with "impl": "reference".
+Multi-GPU (torchrun): every rank multiplies its own replica (replicas only,
+weak scaling); the value is all ranks' products over the max elapsed time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SpGEMM GFLOP/s (2*intermediate products/s), C=A*A, 1 B200"
+KERNELS_PER_MULTIPLY = 1 + 5 + 3 + 5  # analysis, symbolic classes, scan, numeric classes
+
+
+# ----------------------------------------------------------------------------- workloads
+def make_workload(name: str):
+    from research_b200 import matrices as M
+    if name == "rmat20":
+        A = M.rmat(20, 16, (0.57, 0.19, 0.19, 0.05), seed=0)
+        desc = ("R-MAT n=2^20, 16 edges/vertex, probs (0.57,0.19,0.19,0.05), duplicates merged, "
+                "FP64 U[-1,1], seed 0; C=A*A")
+        return A, A, desc
+    if name.startswith("rmat"):
+        sc = int(name[4:])
+        A = M.rmat(sc, 16, (0.57, 0.19, 0.19, 0.05), seed=0)
+        return A, A, f"R-MAT n=2^{sc}, 16 edges/vertex, seed 0; C=A*A"
+    if name == "laplacian256":
+        A = M.laplacian_2d(256, 256, seed=0)
+        return A, A, "2D 5-point Laplacian 256x256, FP64 U[-1,1], seed 0; C=A*A"
+    if name == "rect":
+        A = M.rect_poisson(262144, 1048576, 12.0, seed=0)
+        return A, M.transpose(A), "262144x1048576, Poisson(12)/row, uniform columns, N(0,1), seed 0; C=A*A^T"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def compulsory_bytes(A, B, nnz_c: int) -> int:
+    """Read A once + read B once + write C once (CSR: rowptr + 4 B col + 8 B val)."""
+    w_c = 8 if nnz_c >= 2**32 else 4
+    return (4 * (A.rows + 1) + 12 * A.nnz) + (4 * (B.rows + 1) + 12 * B.nnz) + (w_c * (A.rows + 1) + 12 * nnz_c)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("OCEAN_CLOCKS_CSV", f"/tmp/ocean_clocks_{os.getpid()}.csv"))
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        load = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- CPU leg
+def take_rows(A, rows: np.ndarray):
+    from research_b200.ocean import HostCSR
+    rp = A.rowptr.astype(np.int64)
+    lens = rp[rows + 1] - rp[rows]
+    nrp = np.zeros(rows.size + 1, np.int64)
+    np.cumsum(lens, out=nrp[1:])
+    idx = np.repeat(rp[rows] - nrp[:-1], lens) + np.arange(nrp[-1])
+    return HostCSR(rows.size, A.cols, nrp.astype(np.uint64), A.col[idx], A.val[idx])
+
+
+def cpu_gustavson(A, B, threads: int, chunk_products: int = 300_000_000):
+    """Full CPU Gustavson (symbolic + numeric) of A·B by row chunks into reused
+    buffers; returns (seconds, products, per-row counts)."""
+    from oracle import oracle as O
+    prod, _, _ = O.row_stats(A, B, threads)
+    cum = np.concatenate([[0], np.cumsum(prod.astype(np.int64))])
+    counts = np.empty(A.rows, np.uint64)
+    cj = cx = None
+    t0 = time.perf_counter()
+    r0 = 0
+    while r0 < A.rows:
+        r1 = int(np.searchsorted(cum, cum[r0] + chunk_products, side="right")) - 1
+        r1 = min(max(r1, r0 + 1), A.rows)
+        cnt = O.symbolic(A, B, r0, r1, threads)
+        counts[r0:r1] = cnt
+        cp = np.zeros(r1 - r0 + 1, np.uint64)
+        np.cumsum(cnt, out=cp[1:])
+        n = int(cp[-1])
+        if cj is None or cj.size < n:
+            cj = np.empty(max(n, 1), np.uint32)
+            cx = np.empty(max(n, 1), np.float64)
+        ap = np.ascontiguousarray(A.rowptr, dtype=np.uint64)
+        bp = np.ascontiguousarray(B.rowptr, dtype=np.uint64)
+        rc = O._L().oracle_numeric(A.rows, A.nnz, O._p(ap), O._p(A.col), O._p(A.val), B.rows, B.nnz, O._p(bp),
+                                   O._p(B.col), O._p(B.val), B.cols, r0, r1, O._p(cp), O._p(cj), O._p(cx), 0,
+                                   threads)
+        if rc:
+            raise RuntimeError("oracle_numeric failed")
+        r0 = r1
+    return time.perf_counter() - t0, int(prod.sum()), counts
+
+
+def cpu_sample(A, B, threads: int, target_s: float = 12.0):
+    """Bounded CPU sample: every s-th row of A, s chosen so the run takes about
+    target_s seconds. Returns dict with the measured rate and the sample."""
+    total_rows = A.rows
+    s = 256
+    rows = np.arange(0, total_rows, s)
+    t, p, _ = cpu_gustavson(take_rows(A, rows), B, threads)
+    rate = p / max(t, 1e-6)
+    from oracle import oracle as O
+    prod_all, _, _ = O.row_stats(A, B, threads)
+    total = float(prod_all.sum())
+    frac = min(1.0, target_s * rate / max(total, 1.0))
+    s = max(1, int(round(1.0 / max(frac, 1e-9))))
+    rows = np.arange(0, total_rows, s)
+    sub = take_rows(A, rows)
+    t, p, counts = cpu_gustavson(sub, B, threads)
+    return {"seconds": t, "products": p, "stride": s, "rows": rows, "counts": counts,
+            "gflops": 2.0 * p / t / 1e9}
+
+
+# ----------------------------------------------------------------------------- dist
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------- arms
+def run_reference(args, world, rank):
+    """CPU restatement of the path on the host cores (bounded samples)."""
+    if rank != 0:
+        return
+    A, B, desc = make_workload(args.workload)
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+    prod_all, _, _ = O.row_stats(A, B, threads)
+    total = int(prod_all.sum())
+    # calibrate the stride on a small sample, then time K bounded samples
+    cal = cpu_sample(A, B, threads, target_s=max(2.0, args.ref_seconds))
+    rows = cal["rows"]
+    sub = take_rows(A, rows)
+    for _ in range(max(0, args.warmup - 1)):
+        pass  # the calibration run above is the warm-up
+    times, prods = [], []
+    for _ in range(args.steps):
+        t, p, _ = cpu_gustavson(sub, B, threads)
+        times.append(t)
+        prods.append(p)
+    value = 2.0 * sum(prods) / sum(times) / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GFLOP/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "rows": A.rows, "nnz_A": A.nnz, "products": total},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                         "sample": f"every {cal['stride']}th row of A ({rows.size} rows, {prods[0]} products "
+                                   f"per step), symbolic+numeric OpenMP Gustavson (oracle/gustavson.c)"},
+        "e2e": {"value": round(value, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference has no CPU SpGEMM; this arm times the project's CPU restatement of its "
+                "algorithm on the host cores",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from research_b200.ocean import CsrOut, DeviceCSR, HostCSR, SpGEMM, _check, _ptr, lib
+
+    torch.cuda.set_device(local)
+    A, B, desc = make_workload(args.workload)
+    same = B is A
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    # ---- CPU baseline first (host memory is still free), rank 0 at N=1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(A, B, os.cpu_count() or 1, target_s=args.cpu_seconds)
+
+    # ---- device-resident throughput
+    g = SpGEMM({"track_stage_time": True})
+    dA = DeviceCSR.from_host(A)
+    dB = dA if same else DeviceCSR.from_host(B)
+    for _ in range(args.warmup):
+        C = g.multiply(dA, dB, sptr)
+        C.free(sptr)
+    st0 = g.get_stats()
+    nnz_c = int(st0["C"]["nnz"])
+    products = int(st0["stats"]["intermediate_product"])
+
+    stage_names = ["analysis", "scan"] + [f"symbolic_{c}" for c in ("esc", "hash_s", "hash_m", "hash_l", "bitmap")] \
+        + [f"numeric_{c}" for c in ("esc", "hash_s", "hash_m", "hash_l", "bitmap")]
+    stage_ms = {k: 0.0 for k in stage_names}
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        C = g.multiply(dA, dB, sptr)
+        for k in stage_names:
+            stage_ms[k] += max(g.stage_ms(k), 0.0)
+        C.free(sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    elapsed = max_over_ranks(e0.elapsed_time(e1), world)
+    st = g.get_stats()
+    ms = elapsed / args.steps
+    value = world * 2.0 * products * args.steps / (elapsed / 1e3) / 1e9
+    for k in stage_ms:
+        stage_ms[k] /= args.steps
+
+    # ---- roofline of the dominant kernel
+    peak, peak_kind = measured_peaks()
+    dom = max(stage_ms, key=stage_ms.get)
+    cls = st["classes"]
+    if dom.startswith("numeric_"):
+        c = cls["numeric"][dom[len("numeric_"):]]
+        alg = 12 * c["nnz"] + 12 * c["a_nnz"] + 12 * B.nnz + 8 * c["rows"] + 4 * (B.rows + 1)
+        alg_desc = "12 B x C entries written + 12 B x A entries of its rows + 12 B x nnz(B) + row metadata"
+    elif dom.startswith("symbolic_"):
+        c = cls["symbolic"][dom[len("symbolic_"):]]
+        alg = 4 * c["a_nnz"] + 4 * B.nnz + 4 * (B.rows + 1) + 12 * c["rows"]
+        alg_desc = "4 B x A entries of its rows + 4 B x nnz(B) + row metadata"
+    else:
+        alg = 16 * A.rows
+        alg_desc = "row metadata"
+    achieved = alg / (stage_ms[dom] / 1e3) / 1e9 if stage_ms[dom] > 0 else 0.0
+    traffic = None
+    tfile = ROOT / "profiles" / f"traffic_{args.workload}.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get(dom)
+        except Exception:
+            traffic = None
+    comp = compulsory_bytes(A, B, nnz_c)
+
+    # ---- parity spot check against the oracle (rows of the CPU sample + heavy rows)
+    parity = None
+    if rank == 0 and not args.no_check:
+        from oracle import oracle as O
+        C = g.multiply(dA, dB, sptr)
+        check_rows = [0, 1, 2, A.rows // 2, A.rows - 1] + list(range(3, A.rows, max(1, A.rows // 24)))[:24]
+        worst = 0.0
+        for r in sorted(set(check_rows)):
+            rp, col, val = C.download_rows(r, r + 1)
+            cp, cj, cx, ca = O.spgemm(A, B, r, r + 1, with_abs=True)
+            worst = max(worst, O.compare(rp - rp[0], col, val, cp, cj, cx, ca, 1e-12))
+        counts_ok = None
+        if cpu is not None:
+            rows = cpu["rows"]
+            full = np.empty(A.rows + 1, np.uint64)
+            _check(lib().ocean_csr_download_rows(ctypes.byref(C._out), 0, A.rows, _ptr(full), 0, 0, None))
+            gpu_counts = full[rows + 1] - full[rows]
+            counts_ok = bool(np.array_equal(gpu_counts, cpu["counts"]))
+        C.free(sptr)
+        parity = {"rows_checked_exact": len(set(check_rows)), "max_rel_err": worst, "tolerance": 1e-12,
+                  "cpu_sample_row_counts_equal": counts_ok}
+
+    # ---- end to end through the host-buffer C ABI (pinned inputs, host output)
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, A, B, same, nnz_c, products, world, stream)
+
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "rows": A.rows, "cols": B.cols, "nnz_A": A.nnz, "nnz_B": B.nnz,
+                   "products": products, "nnz_C": nnz_c, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (A is %.0f MB, C %.1f GB)" % (
+                       (12 * A.nnz + 4 * A.rows) / 1e6, 12 * nnz_c / 1e9)},
+        "hbm_gbs_compulsory": round(comp / (ms / 1e3) / 1e9, 2),
+        "gather_gbs_effective": round(12 * products / (ms / 1e3) / 1e9, 2),
+        "stage_ms": {k: round(v, 4) for k, v in stage_ms.items() if v > 0},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "algorithmic_bytes_per_launch": int(alg), "algorithmic_bytes": alg_desc,
+                     "launch_ms": round(stage_ms[dom], 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "cpu_baseline": None if cpu is None else {
+            "value": round(cpu["gflops"], 4), "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"every {cpu['stride']}th row of A ({cpu['rows'].size} rows, {cpu['products']} products), "
+                      f"symbolic+numeric OpenMP Gustavson, {cpu['seconds']:.1f} s"},
+        "e2e": e2e,
+        "gpu_launches": KERNELS_PER_MULTIPLY * args.steps,
+        "clocks": clk,
+        "parity": parity,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, A, B, same, nnz_c, products, world, stream):
+    import torch
+    from research_b200.ocean import CsrOut, CsrView, SpGEMM, _check, lib
+
+    need = 12 * nnz_c + 8 * (A.rows + 1) + 2 * (12 * A.nnz + 8 * A.rows) + (16 << 30)
+    avail = 0
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                avail = int(line.split()[1]) * 1024
+    except Exception:
+        pass
+    if avail and avail < need:
+        return {"value": None, "unit": "GFLOP/s",
+                "note": f"skipped: host has {avail / 2**30:.0f} GiB available, needs {need / 2**30:.0f} GiB"}
+
+    def pinned(a: np.ndarray) -> np.ndarray:
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(a.dtype)[: a.size]
+        v[:] = a
+        pinned.keep.append(t)
+        return v
+    pinned.keep = []
+
+    def pin_csr(m):
+        from research_b200.ocean import HostCSR
+        return HostCSR(m.rows, m.cols, pinned(m.rowptr), pinned(m.col), pinned(m.val))
+
+    pA = pin_csr(A)
+    pB = pA if same else pin_csr(B)
+    g = SpGEMM({})
+    av, bv = pA.view(), pB.view()
+    out = CsrOut()
+    sptr = stream.cuda_stream
+    for _ in range(max(1, min(args.warmup, 2))):  # the first call also pins the host output buffers
+        _check(lib().ocean_spgemm_host(g._h, ctypes.byref(av), ctypes.byref(bv), ctypes.byref(out), sptr))
+    steps = args.e2e_steps or args.steps
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        _check(lib().ocean_spgemm_host(g._h, ctypes.byref(av), ctypes.byref(bv), ctypes.byref(out), sptr))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    elapsed = max_over_ranks(e0.elapsed_time(e1), world)
+    h2d = A.rowptr.nbytes + A.col.nbytes + A.val.nbytes + (0 if same else B.rowptr.nbytes + B.col.nbytes + B.val.nbytes)
+    d2h = (out.rows + 1) * (out.rowptr_bits // 8) + 12 * out.nnz
+    g.close()
+    return {"value": round(world * 2.0 * products * steps / (elapsed / 1e3) / 1e9, 3), "unit": "GFLOP/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": steps,
+            "ms_per_step": round(elapsed / steps, 3),
+            "api": "ocean_spgemm_host (pinned host A/B in, C copied back to pinned host buffers)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat20")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-check", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("note: fewer than 3 warm-up steps", file=sys.stderr)
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

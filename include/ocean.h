@@ -94,6 +94,13 @@ int ocean_csr_free(ocean_csr* C, void* stream);
  * convert(CSR&, const cuCSR&) (src/CSR.cpp:243-250). */
 int ocean_csr_download(const ocean_csr* C, void* rowptr, uint32_t* col, double* val, void* stream);
 
+/* Copy rows [r0, r1) of a result into host buffers: rowptr receives r1-r0+1
+ * absolute offsets (uint64), col/val the entries between them (pass NULL for
+ * both to fetch the row pointers only). Lets a caller inspect part of a result
+ * too large for host memory. */
+int ocean_csr_download_rows(const ocean_csr* C, uint64_t r0, uint64_t r1, uint64_t* rowptr,
+                            uint32_t* col, double* val, void* stream);
+
 /* Exact per-row output counts of A·B (the symbolic phase alone) into the
  * device array row_nnz[A.rows]. Replaces the symbolic kernels' result
  * d_num_outputs_row (kernels/SpGEMM.cuh:759-923). */

@@ -12,6 +12,7 @@ struct DevWork {
   uint32_t* prod = nullptr;      // products per row (saturated to u32)
   uint32_t* lo = nullptr;        // smallest output column per row (kEmpty if none)
   uint32_t* hi = nullptr;        // largest output column per row
+  uint32_t* anz = nullptr;       // entries per row of A
   uint32_t* row_nnz = nullptr;   // exact output count per row
   uint32_t* sym_bins = nullptr;  // [SB_COUNT][rows] row ids per symbolic class
   uint32_t* num_bins = nullptr;  // [NB_COUNT][rows] row ids per numeric class
@@ -37,9 +38,10 @@ template <typename RP>
 void launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
                      cudaStream_t s);
 
+// bin_events (optional): SB_COUNT + 1 events recorded around the class kernels.
 template <typename RP>
 void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms,
-                     cudaStream_t s);
+                     cudaStream_t s, cudaEvent_t* bin_events);
 
 void launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s);
 

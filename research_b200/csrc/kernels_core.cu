@@ -111,9 +111,15 @@ __device__ __forceinline__ int num_bin_for(uint32_t n, uint64_t p, uint64_t span
 template <typename RP, int G>
 __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
                                                   uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
-                                                  uint32_t* __restrict__ row_nnz,
+                                                  uint32_t* __restrict__ anz, uint32_t* __restrict__ row_nnz,
                                                   uint32_t* __restrict__ sym_bins,
                                                   DevCounters* __restrict__ ctr, SymPolicy pol) {
+  __shared__ unsigned long long s_anz[SB_COUNT], s_prod[SB_COUNT];
+  if (threadIdx.x < SB_COUNT) {
+    s_anz[threadIdx.x] = 0ull;
+    s_prod[threadIdx.x] = 0ull;
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int sl = lane & (G - 1);
   const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -146,10 +152,13 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     prod[row] = p > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)p;
     lo[row] = mn;
     hi[row] = mx;
+    anz[row] = (uint32_t)(a1 - a0);
     if (p == 0) {
       row_nnz[row] = 0;
     } else {
       b = sym_bin_for(p, (uint64_t)mx - mn + 1, pol);
+      atomicAdd(&s_anz[b], (unsigned long long)(a1 - a0));
+      atomicAdd(&s_prod[b], p);
     }
   }
   bin_append(b, (uint32_t)row, ctr->sym_count, sym_bins, A.rows);
@@ -164,6 +173,11 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     if (tp) atomicAdd(&ctr->total_products, tp);
     if (mp) atomicMax(&ctr->max_products, mp);
     if (ma) atomicMax(&ctr->max_a_nnz, ma);
+  }
+  __syncthreads();
+  if (threadIdx.x < SB_COUNT) {
+    if (s_anz[threadIdx.x]) atomicAdd(&ctr->sym_anz[threadIdx.x], s_anz[threadIdx.x]);
+    if (s_prod[threadIdx.x]) atomicAdd(&ctr->sym_prod[threadIdx.x], s_prod[threadIdx.x]);
   }
 }
 
@@ -692,9 +706,16 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
                                                      const uint32_t* __restrict__ prod,
                                                      const uint32_t* __restrict__ lo,
                                                      const uint32_t* __restrict__ hi,
+                                                     const uint32_t* __restrict__ anz,
                                                      uint32_t* __restrict__ num_bins,
                                                      DevCounters* __restrict__ ctr, NumPolicy pol) {
   __shared__ unsigned long long scr[33];
+  __shared__ unsigned long long s_cls[NB_COUNT], s_anz[NB_COUNT], s_prod[NB_COUNT];
+  if (threadIdx.x < NB_COUNT) {
+    s_cls[threadIdx.x] = 0ull;
+    s_anz[threadIdx.x] = 0ull;
+    s_prod[threadIdx.x] = 0ull;
+  }
   const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * 4;
   uint32_t v[4];
   unsigned long long s = 0;
@@ -715,8 +736,19 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
       run += v[q];
       const uint32_t p = prod[i];
       b = num_bin_for(v[q], p, (uint64_t)hi[i] - lo[i] + 1, pol);
+      if (b >= 0) {
+        atomicAdd(&s_cls[b], (unsigned long long)v[q]);
+        atomicAdd(&s_anz[b], (unsigned long long)anz[i]);
+        atomicAdd(&s_prod[b], (unsigned long long)p);
+      }
     }
     bin_append(b, (uint32_t)i, ctr->num_count, num_bins, n);
+  }
+  __syncthreads();
+  if (threadIdx.x < NB_COUNT && s_cls[threadIdx.x]) {
+    atomicAdd(&ctr->num_nnz[threadIdx.x], s_cls[threadIdx.x]);
+    atomicAdd(&ctr->num_anz[threadIdx.x], s_anz[threadIdx.x]);
+    atomicAdd(&ctr->num_prod[threadIdx.x], s_prod[threadIdx.x]);
   }
 }
 
@@ -803,26 +835,36 @@ void launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const
   if (avg >= 12.0) {
     const uint64_t threads = A.rows * 32;
     k_analysis<RP, 32><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.row_nnz, w.sym_bins, w.ctr, pol);
+        A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.sym_bins, w.ctr, pol);
   } else {
     const uint64_t threads = A.rows * 4;
     k_analysis<RP, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.row_nnz, w.sym_bins, w.ctr, pol);
+        A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.sym_bins, w.ctr, pol);
   }
 }
 
 template <typename RP>
-void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms, cudaStream_t s) {
+void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms, cudaStream_t s,
+                     cudaEvent_t* ev) {
   if (A.rows == 0) return;
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ev[i], s);
+  };
+  mark(0);
   k_sym_esc<RP><<<num_sms * g_occ[K_SYM_ESC], 256, 0, s>>>(A, B, w.sym_bins, w.ctr, w.row_nnz);
+  mark(1);
   k_sym_hash<RP, 128, 11><<<num_sms * g_occ[K_SYM_S], 128, sym_hash_smem<11>(), s>>>(
       A, B, w.sym_bins, w.ctr, SB_HASH_S, w.prod, w.row_nnz);
+  mark(2);
   k_sym_hash<RP, 256, 13><<<num_sms * g_occ[K_SYM_M], 256, sym_hash_smem<13>(), s>>>(
       A, B, w.sym_bins, w.ctr, SB_HASH_M, w.prod, w.row_nnz);
+  mark(3);
   k_sym_hash<RP, 512, 15><<<num_sms * g_occ[K_SYM_L], 512, sym_hash_smem<15>(), s>>>(
       A, B, w.sym_bins, w.ctr, SB_HASH_L, w.prod, w.row_nnz);
+  mark(4);
   k_sym_bitmap<RP><<<num_sms * g_occ[K_SYM_BM], kBitmapThreads, kSymBitmapSmem, s>>>(
       A, B, w.sym_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz);
+  mark(5);
 }
 
 void launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s) {
@@ -831,7 +873,7 @@ void launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s) {
   k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums);
   k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, w.ctr, w.rowptr64, w.rowptr32, w.rows);
   k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums, w.rowptr64, w.rowptr32,
-                                             w.prod, w.lo, w.hi, w.num_bins, w.ctr, pol);
+                                             w.prod, w.lo, w.hi, w.anz, w.num_bins, w.ctr, pol);
 }
 
 template <typename RP>
@@ -870,9 +912,9 @@ template void launch_analysis<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t
 template void launch_analysis<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
                                         const SymPolicy&, cudaStream_t);
 template void launch_symbolic<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, int,
-                                        cudaStream_t);
+                                        cudaStream_t, cudaEvent_t*);
 template void launch_symbolic<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, int,
-                                        cudaStream_t);
+                                        cudaStream_t, cudaEvent_t*);
 template void launch_numeric<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
                                        uint32_t*, double*, int, cudaStream_t, cudaEvent_t*);
 template void launch_numeric<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,

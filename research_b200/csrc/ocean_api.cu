@@ -56,13 +56,17 @@ struct CResult {
 enum Ev {
   EV_START = 0,
   EV_ANALYSIS,
-  EV_SYMBOLIC,
+  EV_SYM0,  // EV_SYM0 .. EV_SYM0+5: symbolic class boundaries
+  EV_SYMBOLIC = EV_SYM0 + SB_COUNT,
   EV_SCAN,
   EV_NUM0,  // EV_NUM0 .. EV_NUM0+5: numeric class boundaries
-  EV_NUM_END = EV_NUM0 + 5,
+  EV_NUM_END = EV_NUM0 + NB_COUNT,
   EV_END,
   EV_COUNT
 };
+
+const char* const kSymNames[SB_COUNT] = {"esc", "hash_s", "hash_m", "hash_l", "bitmap"};
+const char* const kNumNames[NB_COUNT] = {"esc", "hash_s", "hash_m", "hash_l", "bitmap"};
 
 struct Stats {
   uint64_t a_rows = 0, a_cols = 0, a_nnz = 0, b_rows = 0, b_cols = 0, b_nnz = 0;
@@ -71,6 +75,11 @@ struct Stats {
   uint32_t max_products = 0, max_a_nnz = 0;
   uint32_t sym_bins[SB_COUNT] = {0};
   uint32_t num_bins[NB_COUNT] = {0};
+  uint64_t num_nnz[NB_COUNT] = {0};
+  uint64_t num_anz[NB_COUNT] = {0};
+  uint64_t num_prod[NB_COUNT] = {0};
+  uint64_t sym_anz[SB_COUNT] = {0};
+  uint64_t sym_prod[SB_COUNT] = {0};
   int workflow = 0;  // 0 = precise (symbolic + numeric)
   int rowptr_bits = 32;
   bool valid = false;
@@ -140,8 +149,8 @@ struct ocean_handle {
 
   void free_all() {
     DevWork& x = w;
-    void* ps[] = {x.prod, x.lo, x.hi, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32,
-                  x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
+    void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
+                  x.rowptr32, x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
     for (void* p : ps)
       if (p) cudaFree(p);
     if (h_ctr) cudaFreeHost(h_ctr);
@@ -181,11 +190,12 @@ void ensure_rows(ocean_handle* h, uint64_t rows) {
     return;
   }
   DevWork& x = h->w;
-  void* ps[] = {x.prod, x.lo, x.hi, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32};
+  void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32};
   for (void* p : ps)
     if (p) cudaFree(p);
   const uint64_t r = std::max<uint64_t>(rows, 1);
   OCEAN_CUDA(cudaMalloc((void**)&x.prod, r * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.anz, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.lo, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.hi, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.row_nnz, r * 4));
@@ -259,9 +269,8 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   launch_analysis(A, B, h->w, sp, s);
   OCEAN_CUDA(cudaGetLastError());
   record(h, EV_ANALYSIS, s);
-  launch_symbolic(A, B, h->w, h->num_sms, s);
+  launch_symbolic(A, B, h->w, h->num_sms, s, h->ev + EV_SYM0);
   OCEAN_CUDA(cudaGetLastError());
-  record(h, EV_SYMBOLIC, s);
   if (with_scan) {
     launch_scan(h->w, np, s);
     OCEAN_CUDA(cudaGetLastError());
@@ -339,6 +348,15 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   st.max_a_nnz = h->h_ctr->max_a_nnz;
   for (int i = 0; i < SB_COUNT; ++i) st.sym_bins[i] = h->h_ctr->sym_count[i];
   for (int i = 0; i < NB_COUNT; ++i) st.num_bins[i] = h->h_ctr->num_count[i];
+  for (int i = 0; i < NB_COUNT; ++i) {
+    st.num_nnz[i] = h->h_ctr->num_nnz[i];
+    st.num_anz[i] = h->h_ctr->num_anz[i];
+    st.num_prod[i] = h->h_ctr->num_prod[i];
+  }
+  for (int i = 0; i < SB_COUNT; ++i) {
+    st.sym_anz[i] = h->h_ctr->sym_anz[i];
+    st.sym_prod[i] = h->h_ctr->sym_prod[i];
+  }
   st.rowptr_bits = bits;
   st.workflow = 0;
   st.valid = true;
@@ -405,16 +423,26 @@ std::string stats_json(ocean_handle* h) {
   for (int i = 0; i < SB_COUNT; ++i) o << (i ? ", " : "") << st.sym_bins[i];
   o << "], \"binning_2\": [";
   for (int i = 0; i < NB_COUNT; ++i) o << (i ? ", " : "") << st.num_bins[i];
-  o << "], ";
+  o << "], \"classes\": {\"symbolic\": {";
+  for (int i = 0; i < SB_COUNT; ++i)
+    o << (i ? ", " : "") << "\"" << kSymNames[i] << "\": {\"rows\": " << st.sym_bins[i]
+      << ", \"a_nnz\": " << st.sym_anz[i] << ", \"products\": " << st.sym_prod[i] << "}";
+  o << "}, \"numeric\": {";
+  for (int i = 0; i < NB_COUNT; ++i)
+    o << (i ? ", " : "") << "\"" << kNumNames[i] << "\": {\"rows\": " << st.num_bins[i]
+      << ", \"nnz\": " << st.num_nnz[i] << ", \"a_nnz\": " << st.num_anz[i]
+      << ", \"products\": " << st.num_prod[i] << "}";
+  o << "}}, ";
   const double total = ev_ms(h, EV_START, EV_END);
   if (h->tracked) {
     o << "\"timing\": {\"analysis\": " << ev_ms(h, EV_START, EV_ANALYSIS)
-      << ", \"symbolic\": " << ev_ms(h, EV_ANALYSIS, EV_SYMBOLIC) << ", \"scan\": " << ev_ms(h, EV_SYMBOLIC, EV_SCAN)
-      << ", \"numeric\": " << ev_ms(h, EV_NUM0, EV_NUM_END) << ", \"numeric_esc\": " << ev_ms(h, EV_NUM0, EV_NUM0 + 1)
-      << ", \"numeric_hash_s\": " << ev_ms(h, EV_NUM0 + 1, EV_NUM0 + 2)
-      << ", \"numeric_hash_m\": " << ev_ms(h, EV_NUM0 + 2, EV_NUM0 + 3)
-      << ", \"numeric_hash_l\": " << ev_ms(h, EV_NUM0 + 3, EV_NUM0 + 4)
-      << ", \"numeric_bitmap\": " << ev_ms(h, EV_NUM0 + 4, EV_NUM0 + 5) << ", \"host_ms\": " << st.host_ms << "}, ";
+      << ", \"symbolic\": " << ev_ms(h, EV_SYM0, EV_SYMBOLIC) << ", \"scan\": " << ev_ms(h, EV_SYMBOLIC, EV_SCAN)
+      << ", \"numeric\": " << ev_ms(h, EV_NUM0, EV_NUM_END);
+    for (int i = 0; i < SB_COUNT; ++i)
+      o << ", \"symbolic_" << kSymNames[i] << "\": " << ev_ms(h, EV_SYM0 + i, EV_SYM0 + i + 1);
+    for (int i = 0; i < NB_COUNT; ++i)
+      o << ", \"numeric_" << kNumNames[i] << "\": " << ev_ms(h, EV_NUM0 + i, EV_NUM0 + i + 1);
+    o << ", \"host_ms\": " << st.host_ms << "}, ";
   }
   o << "\"total_time\": " << total << ", \"gflops\": "
     << (total > 0 ? 2.0 * (double)st.total_products / total / 1e6 : 0.0) << "}";
@@ -580,6 +608,34 @@ int ocean_csr_download(const ocean_csr* C, void* rowptr, uint32_t* col, double* 
   });
 }
 
+int ocean_csr_download_rows(const ocean_csr* C, uint64_t r0, uint64_t r1, uint64_t* rowptr, uint32_t* col,
+                            double* val, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(C != nullptr && rowptr != nullptr, OCEAN_ERR_INVALID, "NULL argument");
+    OCEAN_CHECK(r0 <= r1 && r1 <= C->rows, OCEAN_ERR_INVALID, "row range outside C");
+    cudaStream_t s = (cudaStream_t)stream;
+    const cudaMemcpyKind kind = C->location == 1 ? cudaMemcpyHostToHost : cudaMemcpyDeviceToHost;
+    const uint64_t n = r1 - r0 + 1;
+    if (C->rowptr_bits == 64) {
+      OCEAN_CUDA(cudaMemcpyAsync(rowptr, (const uint64_t*)C->rowptr + r0, n * 8, kind, s));
+      OCEAN_CUDA(cudaStreamSynchronize(s));
+    } else {
+      std::vector<uint32_t> tmp(n);
+      OCEAN_CUDA(cudaMemcpyAsync(tmp.data(), (const uint32_t*)C->rowptr + r0, n * 4, kind, s));
+      OCEAN_CUDA(cudaStreamSynchronize(s));
+      for (uint64_t i = 0; i < n; ++i) rowptr[i] = tmp[i];
+    }
+    if (r1 == C->rows) rowptr[n - 1] = C->nnz;
+    const uint64_t b = rowptr[0], e = rowptr[n - 1];
+    OCEAN_CHECK(b <= e && e <= C->nnz, OCEAN_ERR_INTERNAL, "row pointers out of range");
+    if (e > b && col != nullptr && val != nullptr) {
+      OCEAN_CUDA(cudaMemcpyAsync(col, C->col + b, (e - b) * 4, kind, s));
+      OCEAN_CUDA(cudaMemcpyAsync(val, C->val + b, (e - b) * 8, kind, s));
+    }
+    OCEAN_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
 int ocean_symbolic(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, uint32_t* row_nnz,
                    void* stream) {
   return guarded([&] {
@@ -620,14 +676,13 @@ double ocean_stage_ms(ocean_handle* h, const char* stage) {
   if (s == "total") return ev_ms(h, EV_START, EV_END);
   if (!h->tracked) return -1.0;
   if (s == "analysis") return ev_ms(h, EV_START, EV_ANALYSIS);
-  if (s == "symbolic") return ev_ms(h, EV_ANALYSIS, EV_SYMBOLIC);
+  if (s == "symbolic") return ev_ms(h, EV_SYM0, EV_SYMBOLIC);
   if (s == "scan") return ev_ms(h, EV_SYMBOLIC, EV_SCAN);
   if (s == "numeric") return ev_ms(h, EV_NUM0, EV_NUM_END);
-  if (s == "numeric_esc") return ev_ms(h, EV_NUM0, EV_NUM0 + 1);
-  if (s == "numeric_hash_s") return ev_ms(h, EV_NUM0 + 1, EV_NUM0 + 2);
-  if (s == "numeric_hash_m") return ev_ms(h, EV_NUM0 + 2, EV_NUM0 + 3);
-  if (s == "numeric_hash_l") return ev_ms(h, EV_NUM0 + 3, EV_NUM0 + 4);
-  if (s == "numeric_bitmap") return ev_ms(h, EV_NUM0 + 4, EV_NUM0 + 5);
+  for (int i = 0; i < SB_COUNT; ++i)
+    if (s == std::string("symbolic_") + kSymNames[i]) return ev_ms(h, EV_SYM0 + i, EV_SYM0 + i + 1);
+  for (int i = 0; i < NB_COUNT; ++i)
+    if (s == std::string("numeric_") + kNumNames[i]) return ev_ms(h, EV_NUM0 + i, EV_NUM0 + i + 1);
   return -1.0;
 }
 

@@ -47,6 +47,11 @@ struct DevCounters {
   unsigned int sym_cursor[SB_COUNT];
   unsigned int num_count[NB_COUNT];
   unsigned int num_cursor[NB_COUNT];
+  unsigned long long num_nnz[NB_COUNT];   // output entries per numeric class
+  unsigned long long num_anz[NB_COUNT];   // A entries of the rows of each numeric class
+  unsigned long long num_prod[NB_COUNT];  // products of the rows of each numeric class
+  unsigned long long sym_anz[SB_COUNT];   // A entries of the rows of each symbolic class
+  unsigned long long sym_prod[SB_COUNT];  // products of the rows of each symbolic class
   unsigned int status;     // OR of DevError bits
   unsigned int err_row;
   unsigned int pad[4];

@@ -31,7 +31,7 @@ STATUS_NAMES = {0: "OK", 1: "CUDA", 2: "CAPACITY", 3: "TIMEOUT", 4: "INVALID", 5
 # Entry points declared in include/ocean.h (checked by the ABI test).
 EXPORTS = (
     "ocean_create", "ocean_create_from_file", "ocean_destroy", "ocean_spgemm", "ocean_spgemm_host",
-    "ocean_csr_free", "ocean_csr_download", "ocean_symbolic", "ocean_stats_json", "ocean_stage_ms",
+    "ocean_csr_free", "ocean_csr_download", "ocean_csr_download_rows", "ocean_symbolic", "ocean_stats_json", "ocean_stage_ms",
     "ocean_murmur3_u32", "ocean_last_error", "ocean_version",
 )
 
@@ -78,6 +78,7 @@ def lib() -> ctypes.CDLL:
     L.ocean_spgemm_host.argtypes = [vp, P(CsrView), P(CsrView), P(CsrOut), vp]
     L.ocean_csr_free.argtypes = [P(CsrOut), vp]
     L.ocean_csr_download.argtypes = [P(CsrOut), vp, vp, vp, vp]
+    L.ocean_csr_download_rows.argtypes = [P(CsrOut), u64, u64, vp, vp, vp, vp]
     L.ocean_symbolic.argtypes = [vp, P(CsrView), P(CsrView), vp, vp]
     L.ocean_stats_json.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, P(ctypes.c_size_t)]
     L.ocean_stage_ms.argtypes = [vp, ctypes.c_char_p]
@@ -167,6 +168,20 @@ class DeviceCSR:
         val = np.empty(o.nnz, dtype=np.float64)
         _check(lib().ocean_csr_download(ctypes.byref(o), _ptr(rp), _ptr(col), _ptr(val), None))
         return HostCSR(int(o.rows), int(o.cols), rp, col, val)
+
+    def download_rows(self, r0: int, r1: int):
+        """(rowptr u64 absolute, col, val) of rows [r0, r1) of a library result."""
+        o = self._out
+        edge = np.empty(1, np.uint64)
+        _check(lib().ocean_csr_download_rows(ctypes.byref(o), r0, r0, _ptr(edge), 0, 0, None))
+        b = int(edge[0])
+        _check(lib().ocean_csr_download_rows(ctypes.byref(o), r1, r1, _ptr(edge), 0, 0, None))
+        e = int(edge[0])
+        rp = np.empty(r1 - r0 + 1, np.uint64)
+        col = np.empty(max(e - b, 0), np.uint32)
+        val = np.empty(max(e - b, 0), np.float64)
+        _check(lib().ocean_csr_download_rows(ctypes.byref(o), r0, r1, _ptr(rp), _ptr(col), _ptr(val), None))
+        return rp, col, val
 
     def free(self, stream: int = 0) -> None:
         if self._out is not None:
