@@ -301,66 +301,175 @@ __global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, const uin
   }
 }
 
+// ---------------------------------------------------------------- product enumeration
+// Block-wide, load-balanced enumeration of the products of one row of A.
+//
+// The row's A entries are taken in chunks of NT. Each chunk is compacted to its
+// non-empty B rows (one packed block scan gives both the compacted rank and the
+// running product offset), so the chunk's products form one contiguous range
+// [0, total). Every warp takes an equal contiguous slice of that range, 32
+// products per step, lane l handling product base + l. The owning B row of each
+// lane is found without searching: each lane of a 32-row window publishes the
+// bit (incl - base - 1) when its row ends inside the step, one __reduce_or_sync
+// collects the bits, and popc(bits below the lane) is the lane's row offset.
+// UNROLL steps are resolved first and their loads issued together, so every
+// thread keeps UNROLL gathers of B in flight whatever the B-row lengths are.
+template <int NT>
+struct EnumSmem {
+  unsigned long long incl[NT];   // inclusive product offset of each non-empty row
+  unsigned long long bbase[NT];  // B index of the row start minus its product offset
+  double av[NT];                 // A value of the row
+  unsigned long long scan[33];
+};
+
+constexpr int kUnroll = 4;
+
+template <int NT, bool VALS, typename RP, typename Op>
+__device__ __forceinline__ void block_for_each_product(const Csr<RP>& A, const Csr<RP>& B, uint64_t a0,
+                                                       uint64_t a1, EnumSmem<NT>& E, Op&& op) {
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (uint64_t c0 = a0; c0 < a1; c0 += NT) {
+    const uint64_t k = c0 + tid;
+    unsigned long long len = 0, bs = 0;
+    double av = 0.0;
+    if (k < a1) {
+      const uint32_t j = A.col[k];
+      bs = B.row_begin(j);
+      len = B.row_end(j) - bs;
+      if (VALS) av = A.val[k];
+    }
+    // packed scan: high 16 bits count non-empty rows, low 48 bits sum products
+    const unsigned long long packed = len ? ((1ull << 48) | len) : 0ull;
+    unsigned long long tot;
+    const unsigned long long ex = block_excl_scan<NT, unsigned long long>(packed, E.scan, &tot);
+    constexpr unsigned long long kLow = (1ull << 48) - 1;
+    if (len) {
+      const uint32_t r = (uint32_t)(ex >> 48);
+      const unsigned long long off = ex & kLow;
+      E.incl[r] = off + len;
+      E.bbase[r] = bs - off;
+      if (VALS) E.av[r] = av;
+    }
+    const uint32_t nrows = (uint32_t)(tot >> 48);
+    const unsigned long long total = tot & kLow;
+    __syncthreads();
+    const unsigned long long slice = (((total + NW - 1) / NW) + 31) & ~31ull;
+    unsigned long long base = (unsigned long long)warp * slice;
+    const unsigned long long end = min(base + slice, total);
+    if (base < end) {
+      // owner row of product `base`: first row whose inclusive offset exceeds it
+      uint32_t lo = 0, hi = nrows;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (E.incl[mid] <= base) lo = mid + 1; else hi = mid;
+      }
+      uint32_t r_cur = lo;
+      const unsigned lt = lanemask_lt();
+      while (base < end) {
+        unsigned long long bi[kUnroll];
+        uint32_t rr[kUnroll];
+        bool ok[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          const unsigned long long sb = base + (unsigned long long)u * 32;
+          const uint32_t w = r_cur + lane;
+          const unsigned long long inc = w < nrows ? E.incl[w] : ~0ull;
+          const unsigned long long d = inc - sb - 1;
+          const unsigned bit = d < 32 ? (1u << d) : 0u;
+          const unsigned m = __reduce_or_sync(kFull, bit);
+          rr[u] = r_cur + __popc(m & lt);
+          ok[u] = sb + lane < end;
+          bi[u] = ok[u] ? E.bbase[rr[u]] + sb + lane : 0ull;
+          r_cur += __popc(m);
+        }
+        uint32_t c[kUnroll];
+        double bv[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          if (ok[u]) {
+            c[u] = B.col[bi[u]];
+            if (VALS) bv[u] = B.val[bi[u]];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          if (ok[u]) op(c[u], VALS ? E.av[rr[u]] * bv[u] : 0.0);
+        }
+        base += 32 * kUnroll;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------- hash accumulators
 // Symbolic: one block per row, open-addressing set of column ids in shared memory
 // (linear probing, bounded by the table size).
+template <int NT, int LOG2T>
+struct SymHashSmem {
+  uint32_t keys[1 << LOG2T];
+  EnumSmem<NT> e;
+  unsigned long long red[33];
+  uint32_t s_idx;
+};
+
 template <typename RP, int NT, int LOG2T>
 __global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
                                                  DevCounters* __restrict__ ctr, int bin,
                                                  const uint32_t* __restrict__ prod,
                                                  uint32_t* __restrict__ row_nnz) {
   constexpr int T = 1 << LOG2T;
-  extern __shared__ uint32_t keys[];
-  __shared__ unsigned long long red[33];
-  __shared__ uint32_t s_idx;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SymHashSmem<NT, LOG2T>& S = *reinterpret_cast<SymHashSmem<NT, LOG2T>*>(smem_raw);
   const int tid = threadIdx.x;
-  for (int i = tid; i < T; i += NT) keys[i] = kEmpty;
+  for (int i = tid; i < T; i += NT) S.keys[i] = kEmpty;
   const uint32_t count = ctr->sym_count[bin];
   const uint32_t* list = bins + (uint64_t)bin * A.rows;
   for (;;) {
-    if (tid == 0) s_idx = atomicAdd(&ctr->sym_cursor[bin], 1u);
+    if (tid == 0) S.s_idx = atomicAdd(&ctr->sym_cursor[bin], 1u);
     __syncthreads();
-    const uint32_t idx = s_idx;
+    const uint32_t idx = S.s_idx;
     if (idx >= count) break;
     const uint32_t row = list[idx];
-    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
-    const int g = group_size_for(prod[row], a1 - a0);
-    const int gid = tid / g, gl = tid % g, ngr = NT / g;
     unsigned cnt = 0;
     bool full = false;
-    for (uint64_t k = a0 + gid; k < a1; k += ngr) {
-      const uint32_t j = A.col[k];
-      const uint64_t b1 = B.row_end(j);
-      for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
-        const uint32_t c = B.col[q];
-        uint32_t h = hash_slot(c, LOG2T);
-        int probe = 0;
-        for (; probe < T; ++probe) {
-          const uint32_t cur = keys[h];
-          if (cur == c) break;
-          if (cur == kEmpty) {
-            const uint32_t prev = atomicCAS(&keys[h], kEmpty, c);
-            if (prev == kEmpty) {
-              ++cnt;
-              break;
-            }
-            if (prev == c) break;
+    block_for_each_product<NT, false>(A, B, A.row_begin(row), A.row_end(row), S.e, [&](uint32_t c, double) {
+      uint32_t h = hash_slot(c, LOG2T);
+      int probe = 0;
+      for (; probe < T; ++probe) {
+        const uint32_t cur = S.keys[h];
+        if (cur == c) break;
+        if (cur == kEmpty) {
+          const uint32_t prev = atomicCAS(&S.keys[h], kEmpty, c);
+          if (prev == kEmpty) {
+            ++cnt;
+            break;
           }
-          h = (h + 1) & (T - 1);
+          if (prev == c) break;
         }
-        full |= probe == T;
+        h = (h + 1) & (T - 1);
       }
-    }
+      full |= probe == T;
+    });
     if (full) raise_status(ctr, DEV_TABLE_FULL, row);
-    const unsigned long long total = block_sum_u64<NT>(cnt, red);
+    const unsigned long long total = block_sum_u64<NT>(cnt, S.red);
     if (tid == 0) row_nnz[row] = (uint32_t)total;
-    for (int i = tid; i < T; i += NT) keys[i] = kEmpty;
+    for (int i = tid; i < T; i += NT) S.keys[i] = kEmpty;
   }
 }
 
 // Numeric: hash-accumulate FP64 values in shared memory, compact the occupied
 // slots into (column << 32 | slot) keys, bitonic-sort them in shared memory and
 // write the row in column order directly into C.
+template <int NT, int LOG2T>
+struct NumHashSmem {
+  double vals[1 << LOG2T];
+  uint32_t keys[1 << LOG2T];  // reused as (1 << LOG2T) / 2 sort keys of 64 bits
+  EnumSmem<NT> e;
+  uint32_t s_idx, s_n;
+};
+
 template <typename RP, int NT, int LOG2T>
 __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
                                                  DevCounters* __restrict__ ctr, int bin,
@@ -372,70 +481,57 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uin
   constexpr int PER = T / NT;
   constexpr int CAP = T / 2;  // sort capacity (entries) in the reused key area
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* vals = reinterpret_cast<double*>(smem_raw);
-  uint32_t* keys = reinterpret_cast<uint32_t*>(vals + T);
-  unsigned long long* sortbuf = reinterpret_cast<unsigned long long*>(keys);
-  __shared__ uint32_t s_idx, s_n;
+  NumHashSmem<NT, LOG2T>& S = *reinterpret_cast<NumHashSmem<NT, LOG2T>*>(smem_raw);
+  unsigned long long* sortbuf = reinterpret_cast<unsigned long long*>(S.keys);
   const int tid = threadIdx.x;
   for (int i = tid; i < T; i += NT) {
-    keys[i] = kEmpty;
-    vals[i] = 0.0;
+    S.keys[i] = kEmpty;
+    S.vals[i] = 0.0;
   }
   const uint32_t count = ctr->num_count[bin];
   const uint32_t* list = bins + (uint64_t)bin * A.rows;
   for (;;) {
     if (tid == 0) {
-      s_idx = atomicAdd(&ctr->num_cursor[bin], 1u);
-      s_n = 0;
+      S.s_idx = atomicAdd(&ctr->num_cursor[bin], 1u);
+      S.s_n = 0;
     }
     __syncthreads();
-    const uint32_t idx = s_idx;
+    const uint32_t idx = S.s_idx;
     if (idx >= count) break;
     const uint32_t row = list[idx];
-    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
-    const int g = group_size_for(prod[row], a1 - a0);
-    const int gid = tid / g, gl = tid % g, ngr = NT / g;
     bool full = false;
-    for (uint64_t k = a0 + gid; k < a1; k += ngr) {
-      const uint32_t j = A.col[k];
-      const double av = A.val[k];
-      const uint64_t b1 = B.row_end(j);
-      for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
-        const uint32_t c = B.col[q];
-        const double v = av * B.val[q];
-        uint32_t h = hash_slot(c, LOG2T);
-        int probe = 0;
-        for (; probe < T; ++probe) {
-          const uint32_t cur = keys[h];
-          if (cur == c) {
-            atomicAdd(&vals[h], v);
+    block_for_each_product<NT, true>(A, B, A.row_begin(row), A.row_end(row), S.e, [&](uint32_t c, double v) {
+      uint32_t h = hash_slot(c, LOG2T);
+      int probe = 0;
+      for (; probe < T; ++probe) {
+        const uint32_t cur = S.keys[h];
+        if (cur == c) {
+          atomicAdd(&S.vals[h], v);
+          break;
+        }
+        if (cur == kEmpty) {
+          const uint32_t prev = atomicCAS(&S.keys[h], kEmpty, c);
+          if (prev == kEmpty || prev == c) {
+            atomicAdd(&S.vals[h], v);
             break;
           }
-          if (cur == kEmpty) {
-            const uint32_t prev = atomicCAS(&keys[h], kEmpty, c);
-            if (prev == kEmpty || prev == c) {
-              atomicAdd(&vals[h], v);
-              break;
-            }
-          }
-          h = (h + 1) & (T - 1);
         }
-        full |= probe == T;
+        h = (h + 1) & (T - 1);
       }
-    }
+      full |= probe == T;
+    });
     if (full) raise_status(ctr, DEV_TABLE_FULL, row);
-    __syncthreads();
     // compaction: read this thread's slots, then rewrite the key area as sort keys
     uint32_t mine[PER];
     unsigned cnt = 0;
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
-      mine[i] = keys[tid + i * NT];
+      mine[i] = S.keys[tid + i * NT];
       cnt += mine[i] != kEmpty;
     }
-    const unsigned base = cnt ? atomicAdd(&s_n, cnt) : 0u;
+    const unsigned base = cnt ? atomicAdd(&S.s_n, cnt) : 0u;
     __syncthreads();
-    const uint32_t n = s_n;
+    const uint32_t n = S.s_n;
     if (n <= CAP) {
       unsigned w = base;
 #pragma unroll
@@ -473,12 +569,12 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uin
     for (uint32_t i = tid; i < wn; i += NT) {
       const unsigned long long e = sortbuf[i];
       c_col[off + i] = (uint32_t)(e >> 32);
-      c_val[off + i] = vals[(uint32_t)e];
+      c_val[off + i] = S.vals[(uint32_t)e];
     }
     __syncthreads();
     for (int i = tid; i < T; i += NT) {
-      keys[i] = kEmpty;
-      vals[i] = 0.0;
+      S.keys[i] = kEmpty;
+      S.vals[i] = 0.0;
     }
   }
 }
@@ -486,50 +582,48 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uin
 // ---------------------------------------------------------------- bitmap accumulators
 // Symbolic: a bitmap over (a window of) the row's output column span; the count
 // is the popcount. Windows of 2^20 columns sweep wider spans.
+struct BitmapSymSmem {
+  unsigned long long bits[kBitmapWords];
+  EnumSmem<kBitmapThreads> e;
+  unsigned long long red[33];
+  uint32_t s_idx;
+};
+
 template <typename RP>
 __global__ void __launch_bounds__(kBitmapThreads, 1)
     k_sym_bitmap(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins, DevCounters* __restrict__ ctr,
                  const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
                  const uint32_t* __restrict__ hi, uint32_t* __restrict__ row_nnz) {
-  extern __shared__ unsigned long long bits[];
-  __shared__ unsigned long long red[33];
-  __shared__ uint32_t s_idx;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BitmapSymSmem& S = *reinterpret_cast<BitmapSymSmem*>(smem_raw);
   const int tid = threadIdx.x;
-  for (int i = tid; i < kBitmapWords; i += kBitmapThreads) bits[i] = 0ull;
+  for (int i = tid; i < kBitmapWords; i += kBitmapThreads) S.bits[i] = 0ull;
   const uint32_t count = ctr->sym_count[SB_BITMAP];
   const uint32_t* list = bins + (uint64_t)SB_BITMAP * A.rows;
   for (;;) {
-    if (tid == 0) s_idx = atomicAdd(&ctr->sym_cursor[SB_BITMAP], 1u);
+    if (tid == 0) S.s_idx = atomicAdd(&ctr->sym_cursor[SB_BITMAP], 1u);
     __syncthreads();
-    const uint32_t idx = s_idx;
+    const uint32_t idx = S.s_idx;
     if (idx >= count) break;
     const uint32_t row = list[idx];
     const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
-    const int g = group_size_for(prod[row], a1 - a0);
-    const int gid = tid / g, gl = tid % g, ngr = kBitmapThreads / g;
     const uint64_t rlo = lo[row], rhi = hi[row];
     unsigned long long total = 0;
     for (uint64_t w0 = rlo; w0 <= rhi; w0 += kBitmapBits) {
       const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
       const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
-      for (uint64_t k = a0 + gid; k < a1; k += ngr) {
-        const uint32_t j = A.col[k];
-        const uint64_t b1 = B.row_end(j);
-        for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
-          const uint64_t c = B.col[q];
-          if (c >= w0 && c < w1) {
-            const uint32_t d = (uint32_t)(c - w0);
-            atomicOr(&bits[d >> 6], 1ull << (d & 63));
-          }
+      block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, [&](uint32_t c, double) {
+        if (c >= w0 && c < w1) {
+          const uint32_t d = (uint32_t)(c - w0);
+          atomicOr(&S.bits[d >> 6], 1ull << (d & 63));
         }
-      }
-      __syncthreads();
+      });
       unsigned long long cnt = 0;
       for (uint32_t w = tid; w < nwords; w += kBitmapThreads) {
-        cnt += __popcll(bits[w]);
-        bits[w] = 0ull;
+        cnt += __popcll(S.bits[w]);
+        S.bits[w] = 0ull;
       }
-      total += block_sum_u64<kBitmapThreads>(cnt, red);
+      total += block_sum_u64<kBitmapThreads>(cnt, S.red);
     }
     if (tid == 0) row_nnz[row] = (uint32_t)total;
   }
@@ -546,6 +640,7 @@ struct BitmapNumSmem {
   uint16_t wpre[kBitmapWords];
   uint32_t spre[kSupers];
   uint32_t scan[33];
+  EnumSmem<kBitmapThreads> e;
   uint32_t s_idx;
 };
 
@@ -569,8 +664,6 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     if (idx >= count) break;
     const uint32_t row = list[idx];
     const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
-    const int g = group_size_for(prod[row], a1 - a0);
-    const int gid = tid / g, gl = tid % g, ngr = kBitmapThreads / g;
     const uint64_t rlo = lo[row], rhi = hi[row];
     const uint64_t row_off = rowptr[row];
     const uint32_t expect = row_nnz[row];
@@ -580,18 +673,12 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
       const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
       // pass 1: mark columns
-      for (uint64_t k = a0 + gid; k < a1; k += ngr) {
-        const uint32_t j = A.col[k];
-        const uint64_t b1 = B.row_end(j);
-        for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
-          const uint64_t c = B.col[q];
-          if (c >= w0 && c < w1) {
-            const uint32_t d = (uint32_t)(c - w0);
-            atomicOr(&S.bits[d >> 6], 1ull << (d & 63));
-          }
+      block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, [&](uint32_t c, double) {
+        if (c >= w0 && c < w1) {
+          const uint32_t d = (uint32_t)(c - w0);
+          atomicOr(&S.bits[d >> 6], 1ull << (d & 63));
         }
-      }
-      __syncthreads();
+      });
       // rank table: thread t owns words [16t, 16t+16)
       const uint32_t wbeg = (uint32_t)tid * kWordsPerThread;
       uint32_t local = 0;
@@ -628,22 +715,14 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       }
       __syncthreads();
       // pass 2: accumulate values at their ranks
-      for (uint64_t k = a0 + gid; k < a1; k += ngr) {
-        const uint32_t j = A.col[k];
-        const double av = A.val[k];
-        const uint64_t b1 = B.row_end(j);
-        for (uint64_t q = B.row_begin(j) + gl; q < b1; q += g) {
-          const uint64_t c = B.col[q];
-          if (c >= w0 && c < w1) {
-            const uint32_t d = (uint32_t)(c - w0);
-            const uint32_t w = d >> 6;
-            const uint32_t r = S.spre[w >> 10] + S.wpre[w] +
-                               __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));
-            if (off + r < row_lim) atomicAdd(&c_val[off + r], av * B.val[q]);
-          }
+      block_for_each_product<kBitmapThreads, true>(A, B, a0, a1, S.e, [&](uint32_t c, double v) {
+        if (c >= w0 && c < w1) {
+          const uint32_t d = (uint32_t)(c - w0);
+          const uint32_t w = d >> 6;
+          const uint32_t r = S.spre[w >> 10] + S.wpre[w] + __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));
+          if (off + r < row_lim) atomicAdd(&c_val[off + r], v);
         }
-      }
-      __syncthreads();
+      });
 #pragma unroll
       for (int i = 0; i < kWordsPerThread; ++i) {
         const uint32_t w = wbeg + i;
@@ -781,11 +860,11 @@ __global__ void k_murmur3(const uint32_t* __restrict__ keys, uint32_t* __restric
 // ---------------------------------------------------------------- launchers
 namespace {
 constexpr size_t kNumBitmapSmem = sizeof(BitmapNumSmem);
-constexpr size_t kSymBitmapSmem = sizeof(unsigned long long) * kBitmapWords;
-template <int LOG2T>
-constexpr size_t num_hash_smem() { return (size_t)(1 << LOG2T) * 12; }
-template <int LOG2T>
-constexpr size_t sym_hash_smem() { return (size_t)(1 << LOG2T) * 4; }
+constexpr size_t kSymBitmapSmem = sizeof(BitmapSymSmem);
+template <int NT, int LOG2T>
+constexpr size_t num_hash_smem() { return sizeof(NumHashSmem<NT, LOG2T>); }
+template <int NT, int LOG2T>
+constexpr size_t sym_hash_smem() { return sizeof(SymHashSmem<NT, LOG2T>); }
 
 int g_occ[16];  // resident blocks per SM of each persistent kernel (same order as kinds)
 enum Kind { K_SYM_ESC, K_SYM_S, K_SYM_M, K_SYM_L, K_SYM_BM, K_NUM_ESC, K_NUM_S, K_NUM_M, K_NUM_L, K_NUM_BM };
@@ -797,18 +876,21 @@ int occ_of(F f, int threads, size_t smem) {
   return n;
 }
 
+template <typename K>
+void allow_smem(K k, size_t bytes) {
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 template <typename RP>
 void set_attrs() {
-  cudaFuncSetAttribute(k_sym_bitmap<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSymBitmapSmem);
-  cudaFuncSetAttribute(k_num_bitmap<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNumBitmapSmem);
-  cudaFuncSetAttribute(k_sym_hash<RP, 512, 15>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sym_hash_smem<15>());
-  cudaFuncSetAttribute(k_sym_hash<RP, 256, 13>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sym_hash_smem<13>());
-  cudaFuncSetAttribute(k_num_hash<RP, 512, 13>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)num_hash_smem<13>());
-  cudaFuncSetAttribute(k_num_hash<RP, 256, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)num_hash_smem<12>());
+  allow_smem(k_sym_bitmap<RP>, kSymBitmapSmem);
+  allow_smem(k_num_bitmap<RP>, kNumBitmapSmem);
+  allow_smem(k_sym_hash<RP, 128, 11>, sym_hash_smem<128, 11>());
+  allow_smem(k_sym_hash<RP, 256, 13>, sym_hash_smem<256, 13>());
+  allow_smem(k_sym_hash<RP, 512, 15>, sym_hash_smem<512, 15>());
+  allow_smem(k_num_hash<RP, 128, 10>, num_hash_smem<128, 10>());
+  allow_smem(k_num_hash<RP, 256, 12>, num_hash_smem<256, 12>());
+  allow_smem(k_num_hash<RP, 512, 13>, num_hash_smem<512, 13>());
 }
 }  // namespace
 
@@ -816,14 +898,14 @@ void configure_kernel_attributes() {
   set_attrs<uint32_t>();
   set_attrs<uint64_t>();
   g_occ[K_SYM_ESC] = occ_of(k_sym_esc<uint32_t>, 256, 0);
-  g_occ[K_SYM_S] = occ_of(k_sym_hash<uint32_t, 128, 11>, 128, sym_hash_smem<11>());
-  g_occ[K_SYM_M] = occ_of(k_sym_hash<uint32_t, 256, 13>, 256, sym_hash_smem<13>());
-  g_occ[K_SYM_L] = occ_of(k_sym_hash<uint32_t, 512, 15>, 512, sym_hash_smem<15>());
+  g_occ[K_SYM_S] = occ_of(k_sym_hash<uint32_t, 128, 11>, 128, sym_hash_smem<128, 11>());
+  g_occ[K_SYM_M] = occ_of(k_sym_hash<uint32_t, 256, 13>, 256, sym_hash_smem<256, 13>());
+  g_occ[K_SYM_L] = occ_of(k_sym_hash<uint32_t, 512, 15>, 512, sym_hash_smem<512, 15>());
   g_occ[K_SYM_BM] = occ_of(k_sym_bitmap<uint32_t>, kBitmapThreads, kSymBitmapSmem);
   g_occ[K_NUM_ESC] = occ_of(k_num_esc<uint32_t>, 256, 0);
-  g_occ[K_NUM_S] = occ_of(k_num_hash<uint32_t, 128, 10>, 128, num_hash_smem<10>());
-  g_occ[K_NUM_M] = occ_of(k_num_hash<uint32_t, 256, 12>, 256, num_hash_smem<12>());
-  g_occ[K_NUM_L] = occ_of(k_num_hash<uint32_t, 512, 13>, 512, num_hash_smem<13>());
+  g_occ[K_NUM_S] = occ_of(k_num_hash<uint32_t, 128, 10>, 128, num_hash_smem<128, 10>());
+  g_occ[K_NUM_M] = occ_of(k_num_hash<uint32_t, 256, 12>, 256, num_hash_smem<256, 12>());
+  g_occ[K_NUM_L] = occ_of(k_num_hash<uint32_t, 512, 13>, 512, num_hash_smem<512, 13>());
   g_occ[K_NUM_BM] = occ_of(k_num_bitmap<uint32_t>, kBitmapThreads, kNumBitmapSmem);
 }
 
@@ -853,13 +935,13 @@ void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int n
   mark(0);
   k_sym_esc<RP><<<num_sms * g_occ[K_SYM_ESC], 256, 0, s>>>(A, B, w.sym_bins, w.ctr, w.row_nnz);
   mark(1);
-  k_sym_hash<RP, 128, 11><<<num_sms * g_occ[K_SYM_S], 128, sym_hash_smem<11>(), s>>>(
+  k_sym_hash<RP, 128, 11><<<num_sms * g_occ[K_SYM_S], 128, sym_hash_smem<128, 11>(), s>>>(
       A, B, w.sym_bins, w.ctr, SB_HASH_S, w.prod, w.row_nnz);
   mark(2);
-  k_sym_hash<RP, 256, 13><<<num_sms * g_occ[K_SYM_M], 256, sym_hash_smem<13>(), s>>>(
+  k_sym_hash<RP, 256, 13><<<num_sms * g_occ[K_SYM_M], 256, sym_hash_smem<256, 13>(), s>>>(
       A, B, w.sym_bins, w.ctr, SB_HASH_M, w.prod, w.row_nnz);
   mark(3);
-  k_sym_hash<RP, 512, 15><<<num_sms * g_occ[K_SYM_L], 512, sym_hash_smem<15>(), s>>>(
+  k_sym_hash<RP, 512, 15><<<num_sms * g_occ[K_SYM_L], 512, sym_hash_smem<512, 15>(), s>>>(
       A, B, w.sym_bins, w.ctr, SB_HASH_L, w.prod, w.row_nnz);
   mark(4);
   k_sym_bitmap<RP><<<num_sms * g_occ[K_SYM_BM], kBitmapThreads, kSymBitmapSmem, s>>>(
@@ -887,13 +969,13 @@ void launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32
   k_num_esc<RP><<<num_sms * g_occ[K_NUM_ESC], 256, 0, s>>>(A, B, w.num_bins, w.ctr, w.row_nnz,
                                                             w.rowptr64, c_col, c_val);
   mark(1);
-  k_num_hash<RP, 128, 10><<<num_sms * g_occ[K_NUM_S], 128, num_hash_smem<10>(), s>>>(
+  k_num_hash<RP, 128, 10><<<num_sms * g_occ[K_NUM_S], 128, num_hash_smem<128, 10>(), s>>>(
       A, B, w.num_bins, w.ctr, NB_HASH_S, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
   mark(2);
-  k_num_hash<RP, 256, 12><<<num_sms * g_occ[K_NUM_M], 256, num_hash_smem<12>(), s>>>(
+  k_num_hash<RP, 256, 12><<<num_sms * g_occ[K_NUM_M], 256, num_hash_smem<256, 12>(), s>>>(
       A, B, w.num_bins, w.ctr, NB_HASH_M, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
   mark(3);
-  k_num_hash<RP, 512, 13><<<num_sms * g_occ[K_NUM_L], 512, num_hash_smem<13>(), s>>>(
+  k_num_hash<RP, 512, 13><<<num_sms * g_occ[K_NUM_L], 512, num_hash_smem<512, 13>(), s>>>(
       A, B, w.num_bins, w.ctr, NB_HASH_L, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
   mark(4);
   k_num_bitmap<RP><<<num_sms * g_occ[K_NUM_BM], kBitmapThreads, kNumBitmapSmem, s>>>(
