@@ -51,6 +51,13 @@ def make_workload(name: str):
         desc = ("R-MAT n=2^20, 16 edges/vertex, probs (0.57,0.19,0.19,0.05), duplicates merged, "
                 "FP64 U[-1,1], seed 0; C=A*A")
         return A, A, desc
+    if name == "rmat20h":
+        # profiling case: every 64th heavy row (> 16384 products) of the R-MAT 2^20 workload times A
+        from oracle import oracle as O
+        A = M.rmat(20, 16, (0.57, 0.19, 0.19, 0.05), seed=0)
+        p, _, _ = O.row_stats(A, A)
+        rows = np.nonzero(p > 16384)[0][::64]
+        return take_rows(A, rows), A, f"{rows.size} heavy rows of R-MAT n=2^20 (every 64th with >16384 products) times A"
     if name.startswith("rmat"):
         sc = int(name[4:])
         A = M.rmat(sc, 16, (0.57, 0.19, 0.19, 0.05), seed=0)

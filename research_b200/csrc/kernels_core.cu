@@ -320,86 +320,128 @@ struct EnumSmem {
   unsigned long long bbase[NT];  // B index of the row start minus its product offset
   double av[NT];                 // A value of the row
   unsigned long long scan[33];
+  unsigned long long total;      // products of the loaded chunk
+  uint32_t nrows;                // non-empty rows of the loaded chunk
 };
 
 constexpr int kUnroll = 4;
 
+// Loads A entries [c0, min(c0 + NT, a1)) into E (compacted to non-empty B rows).
+template <int NT, bool VALS, typename RP>
+__device__ __forceinline__ void block_load_chunk(const Csr<RP>& A, const Csr<RP>& B, uint64_t c0, uint64_t a1,
+                                                 EnumSmem<NT>& E) {
+  const int tid = threadIdx.x;
+  const uint64_t k = c0 + tid;
+  unsigned long long len = 0, bs = 0;
+  double av = 0.0;
+  if (k < a1) {
+    const uint32_t j = A.col[k];
+    bs = B.row_begin(j);
+    len = B.row_end(j) - bs;
+    if (VALS) av = A.val[k];
+  }
+  // packed scan: high 16 bits count non-empty rows, low 48 bits sum products
+  const unsigned long long packed = len ? ((1ull << 48) | len) : 0ull;
+  unsigned long long tot;
+  const unsigned long long ex = block_excl_scan<NT, unsigned long long>(packed, E.scan, &tot);
+  constexpr unsigned long long kLow = (1ull << 48) - 1;
+  if (len) {
+    const uint32_t r = (uint32_t)(ex >> 48);
+    const unsigned long long off = ex & kLow;
+    E.incl[r] = off + len;
+    E.bbase[r] = bs - off;
+    if (VALS) E.av[r] = av;
+  }
+  if (tid == 0) {
+    E.nrows = (uint32_t)(tot >> 48);
+    E.total = tot & kLow;
+  }
+  __syncthreads();
+}
+
+// Enumerates the products of the chunk held in E. `op(col, value, ok)` is
+// called by all 32 lanes of a warp together (ok = false for idle lanes), so it
+// may use warp-collective operations.
+template <int NT, bool VALS, typename RP, typename Op>
+__device__ __forceinline__ void block_run_chunk(const Csr<RP>& B, EnumSmem<NT>& E, Op&& op) {
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t nrows = E.nrows;
+  const unsigned long long total = E.total;
+  const unsigned long long slice = (((total + NW - 1) / NW) + 31) & ~31ull;
+  unsigned long long base = (unsigned long long)warp * slice;
+  const unsigned long long end = min(base + slice, total);
+  if (base < end) {
+    // owner row of product `base`: first row whose inclusive offset exceeds it
+    uint32_t lo = 0, hi = nrows;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (E.incl[mid] <= base) lo = mid + 1; else hi = mid;
+    }
+    uint32_t r_cur = lo;
+    const unsigned lt = lanemask_lt();
+    while (base < end) {
+      unsigned long long bi[kUnroll];
+      uint32_t rr[kUnroll];
+      bool ok[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const unsigned long long sb = base + (unsigned long long)u * 32;
+        const uint32_t w = r_cur + lane;
+        const unsigned long long inc = w < nrows ? E.incl[w] : ~0ull;
+        const unsigned long long d = inc - sb - 1;
+        const unsigned bit = d < 32 ? (1u << d) : 0u;
+        const unsigned m = __reduce_or_sync(kFull, bit);
+        rr[u] = r_cur + __popc(m & lt);
+        ok[u] = sb + lane < end;
+        bi[u] = ok[u] ? E.bbase[rr[u]] + sb + lane : 0ull;
+        r_cur += __popc(m);
+      }
+      uint32_t c[kUnroll];
+      double bv[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        c[u] = kEmpty;
+        bv[u] = 0.0;
+        if (ok[u]) {
+          c[u] = B.col[bi[u]];
+          if (VALS) bv[u] = B.val[bi[u]];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) op(c[u], (VALS && ok[u]) ? E.av[rr[u]] * bv[u] : 0.0, ok[u]);
+      base += 32 * kUnroll;
+    }
+  }
+  __syncthreads();
+}
+
+// Enumerates every product of A entries [a0, a1) (all chunks).
 template <int NT, bool VALS, typename RP, typename Op>
 __device__ __forceinline__ void block_for_each_product(const Csr<RP>& A, const Csr<RP>& B, uint64_t a0,
                                                        uint64_t a1, EnumSmem<NT>& E, Op&& op) {
-  constexpr int NW = NT / 32;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (uint64_t c0 = a0; c0 < a1; c0 += NT) {
-    const uint64_t k = c0 + tid;
-    unsigned long long len = 0, bs = 0;
-    double av = 0.0;
-    if (k < a1) {
-      const uint32_t j = A.col[k];
-      bs = B.row_begin(j);
-      len = B.row_end(j) - bs;
-      if (VALS) av = A.val[k];
-    }
-    // packed scan: high 16 bits count non-empty rows, low 48 bits sum products
-    const unsigned long long packed = len ? ((1ull << 48) | len) : 0ull;
-    unsigned long long tot;
-    const unsigned long long ex = block_excl_scan<NT, unsigned long long>(packed, E.scan, &tot);
-    constexpr unsigned long long kLow = (1ull << 48) - 1;
-    if (len) {
-      const uint32_t r = (uint32_t)(ex >> 48);
-      const unsigned long long off = ex & kLow;
-      E.incl[r] = off + len;
-      E.bbase[r] = bs - off;
-      if (VALS) E.av[r] = av;
-    }
-    const uint32_t nrows = (uint32_t)(tot >> 48);
-    const unsigned long long total = tot & kLow;
-    __syncthreads();
-    const unsigned long long slice = (((total + NW - 1) / NW) + 31) & ~31ull;
-    unsigned long long base = (unsigned long long)warp * slice;
-    const unsigned long long end = min(base + slice, total);
-    if (base < end) {
-      // owner row of product `base`: first row whose inclusive offset exceeds it
-      uint32_t lo = 0, hi = nrows;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (E.incl[mid] <= base) lo = mid + 1; else hi = mid;
-      }
-      uint32_t r_cur = lo;
-      const unsigned lt = lanemask_lt();
-      while (base < end) {
-        unsigned long long bi[kUnroll];
-        uint32_t rr[kUnroll];
-        bool ok[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          const unsigned long long sb = base + (unsigned long long)u * 32;
-          const uint32_t w = r_cur + lane;
-          const unsigned long long inc = w < nrows ? E.incl[w] : ~0ull;
-          const unsigned long long d = inc - sb - 1;
-          const unsigned bit = d < 32 ? (1u << d) : 0u;
-          const unsigned m = __reduce_or_sync(kFull, bit);
-          rr[u] = r_cur + __popc(m & lt);
-          ok[u] = sb + lane < end;
-          bi[u] = ok[u] ? E.bbase[rr[u]] + sb + lane : 0ull;
-          r_cur += __popc(m);
-        }
-        uint32_t c[kUnroll];
-        double bv[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          if (ok[u]) {
-            c[u] = B.col[bi[u]];
-            if (VALS) bv[u] = B.val[bi[u]];
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          if (ok[u]) op(c[u], VALS ? E.av[rr[u]] * bv[u] : 0.0);
-        }
-        base += 32 * kUnroll;
-      }
-    }
-    __syncthreads();
+    block_load_chunk<NT, VALS>(A, B, c0, a1, E);
+    block_run_chunk<NT, VALS>(B, E, op);
+  }
+}
+
+// Sets the bit of column c (relative to w0, inside [w0, w1)) with one
+// shared-memory atomic per distinct 64-bit word per warp step: lanes hitting the
+// same word OR their bits together first, and the word is only written when a
+// bit is still missing.
+__device__ __forceinline__ void warp_mark_bit(unsigned long long* bits, uint32_t c, bool ok, uint64_t w0,
+                                              uint64_t w1) {
+  const bool in = ok && c >= w0 && c < w1;
+  const uint32_t d = in ? (uint32_t)(c - w0) : 0u;
+  const uint32_t word = in ? (d >> 6) : kEmpty;
+  const unsigned peers = __match_any_sync(kFull, word);
+  const unsigned long long bit = in ? (1ull << (d & 63)) : 0ull;
+  const unsigned lo = __reduce_or_sync(peers, (unsigned)bit);
+  const unsigned hi = __reduce_or_sync(peers, (unsigned)(bit >> 32));
+  if (in && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) {
+    const unsigned long long m = ((unsigned long long)hi << 32) | lo;
+    if ((bits[word] & m) != m) atomicOr(&bits[word], m);
   }
 }
 
@@ -434,7 +476,8 @@ __global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, const uin
     const uint32_t row = list[idx];
     unsigned cnt = 0;
     bool full = false;
-    block_for_each_product<NT, false>(A, B, A.row_begin(row), A.row_end(row), S.e, [&](uint32_t c, double) {
+    block_for_each_product<NT, false>(A, B, A.row_begin(row), A.row_end(row), S.e, [&](uint32_t c, double, bool ok) {
+      if (!ok) return;
       uint32_t h = hash_slot(c, LOG2T);
       int probe = 0;
       for (; probe < T; ++probe) {
@@ -500,7 +543,8 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uin
     if (idx >= count) break;
     const uint32_t row = list[idx];
     bool full = false;
-    block_for_each_product<NT, true>(A, B, A.row_begin(row), A.row_end(row), S.e, [&](uint32_t c, double v) {
+    block_for_each_product<NT, true>(A, B, A.row_begin(row), A.row_end(row), S.e, [&](uint32_t c, double v, bool ok) {
+      if (!ok) return;
       uint32_t h = hash_slot(c, LOG2T);
       int probe = 0;
       for (; probe < T; ++probe) {
@@ -612,11 +656,8 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     for (uint64_t w0 = rlo; w0 <= rhi; w0 += kBitmapBits) {
       const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
       const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
-      block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, [&](uint32_t c, double) {
-        if (c >= w0 && c < w1) {
-          const uint32_t d = (uint32_t)(c - w0);
-          atomicOr(&S.bits[d >> 6], 1ull << (d & 63));
-        }
+      block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, [&](uint32_t c, double, bool ok) {
+        warp_mark_bit(S.bits, c, ok, w0, w1);
       });
       unsigned long long cnt = 0;
       for (uint32_t w = tid; w < nwords; w += kBitmapThreads) {
@@ -669,16 +710,16 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     const uint32_t expect = row_nnz[row];
     const uint64_t row_lim = row_off + expect;
     uint64_t off = row_off;
+    // a row whose A entries fit one chunk is loaded once for both passes
+    const bool one_chunk = a1 - a0 <= (uint64_t)kBitmapThreads;
+    if (one_chunk) block_load_chunk<kBitmapThreads, true>(A, B, a0, a1, S.e);
     for (uint64_t w0 = rlo; w0 <= rhi; w0 += kBitmapBits) {
       const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
       const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
       // pass 1: mark columns
-      block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, [&](uint32_t c, double) {
-        if (c >= w0 && c < w1) {
-          const uint32_t d = (uint32_t)(c - w0);
-          atomicOr(&S.bits[d >> 6], 1ull << (d & 63));
-        }
-      });
+      auto mark = [&](uint32_t c, double, bool ok) { warp_mark_bit(S.bits, c, ok, w0, w1); };
+      if (one_chunk) block_run_chunk<kBitmapThreads, false>(B, S.e, mark);
+      else block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, mark);
       // rank table: thread t owns words [16t, 16t+16)
       const uint32_t wbeg = (uint32_t)tid * kWordsPerThread;
       uint32_t local = 0;
@@ -715,14 +756,16 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       }
       __syncthreads();
       // pass 2: accumulate values at their ranks
-      block_for_each_product<kBitmapThreads, true>(A, B, a0, a1, S.e, [&](uint32_t c, double v) {
-        if (c >= w0 && c < w1) {
+      auto accumulate = [&](uint32_t c, double v, bool ok) {
+        if (ok && c >= w0 && c < w1) {
           const uint32_t d = (uint32_t)(c - w0);
           const uint32_t w = d >> 6;
           const uint32_t r = S.spre[w >> 10] + S.wpre[w] + __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));
           if (off + r < row_lim) atomicAdd(&c_val[off + r], v);
         }
-      });
+      };
+      if (one_chunk) block_run_chunk<kBitmapThreads, true>(B, S.e, accumulate);
+      else block_for_each_product<kBitmapThreads, true>(A, B, a0, a1, S.e, accumulate);
 #pragma unroll
       for (int i = 0; i < kWordsPerThread; ++i) {
         const uint32_t w = wbeg + i;
