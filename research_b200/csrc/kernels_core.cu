@@ -324,7 +324,10 @@ struct EnumSmem {
   uint32_t nrows;                // non-empty rows of the loaded chunk
 };
 
-constexpr int kUnroll = 4;
+#ifndef OCEAN_UNROLL
+#define OCEAN_UNROLL 4
+#endif
+constexpr int kUnroll = OCEAN_UNROLL;  // gathers in flight per thread in the product enumeration
 
 // Loads A entries [c0, min(c0 + NT, a1)) into E (compacted to non-empty B rows).
 template <int NT, bool VALS, typename RP>
@@ -360,11 +363,13 @@ __device__ __forceinline__ void block_load_chunk(const Csr<RP>& A, const Csr<RP>
 }
 
 // Enumerates the products of the chunk held in E. `op(col, value, ok)` is
-// called by all 32 lanes of a warp together (ok = false for idle lanes), so it
-// may use warp-collective operations.
+// called by all 32 lanes of a warp together (ok = false for idle lanes).
+// Fast path: while the warp's next kUnroll steps all lie inside one B row, the
+// lanes issue plain strided gathers of that row (no owner search).
 template <int NT, bool VALS, typename RP, typename Op>
 __device__ __forceinline__ void block_run_chunk(const Csr<RP>& B, EnumSmem<NT>& E, Op&& op) {
   constexpr int NW = NT / 32;
+  constexpr unsigned long long kSpan = 32ull * kUnroll;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t nrows = E.nrows;
   const unsigned long long total = E.total;
@@ -381,6 +386,22 @@ __device__ __forceinline__ void block_run_chunk(const Csr<RP>& B, EnumSmem<NT>& 
     uint32_t r_cur = lo;
     const unsigned lt = lanemask_lt();
     while (base < end) {
+      while (E.incl[r_cur] <= base) ++r_cur;
+      if (E.incl[r_cur] >= base + kSpan && end >= base + kSpan) {
+        const unsigned long long b0 = E.bbase[r_cur] + base + lane;
+        const double av = VALS ? E.av[r_cur] : 0.0;
+        uint32_t c[kUnroll];
+        double bv[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          c[u] = B.col[b0 + 32 * u];
+          if (VALS) bv[u] = B.val[b0 + 32 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) op(c[u], VALS ? av * bv[u] : 0.0, true);
+        base += kSpan;
+        continue;
+      }
       unsigned long long bi[kUnroll];
       uint32_t rr[kUnroll];
       bool ok[kUnroll];
@@ -410,7 +431,7 @@ __device__ __forceinline__ void block_run_chunk(const Csr<RP>& B, EnumSmem<NT>& 
       }
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) op(c[u], (VALS && ok[u]) ? E.av[rr[u]] * bv[u] : 0.0, ok[u]);
-      base += 32 * kUnroll;
+      base += kSpan;
     }
   }
   __syncthreads();
@@ -426,22 +447,16 @@ __device__ __forceinline__ void block_for_each_product(const Csr<RP>& A, const C
   }
 }
 
-// Sets the bit of column c (relative to w0, inside [w0, w1)) with one
-// shared-memory atomic per distinct 64-bit word per warp step: lanes hitting the
-// same word OR their bits together first, and the word is only written when a
-// bit is still missing.
-__device__ __forceinline__ void warp_mark_bit(unsigned long long* bits, uint32_t c, bool ok, uint64_t w0,
-                                              uint64_t w1) {
-  const bool in = ok && c >= w0 && c < w1;
-  const uint32_t d = in ? (uint32_t)(c - w0) : 0u;
-  const uint32_t word = in ? (d >> 6) : kEmpty;
-  const unsigned peers = __match_any_sync(kFull, word);
-  const unsigned long long bit = in ? (1ull << (d & 63)) : 0ull;
-  const unsigned lo = __reduce_or_sync(peers, (unsigned)bit);
-  const unsigned hi = __reduce_or_sync(peers, (unsigned)(bit >> 32));
-  if (in && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) {
-    const unsigned long long m = ((unsigned long long)hi << 32) | lo;
-    if ((bits[word] & m) != m) atomicOr(&bits[word], m);
+// Sets the bit of column c of the window [w0, w1) (`single`: the window
+// holds the whole row, no range test). The word is read first and only
+// written by an atomic when the bit is still clear, so hot columns that are
+// already marked cost one shared-memory load.
+__device__ __forceinline__ void mark_bit(unsigned long long* bits, uint32_t c, bool ok, bool single, uint64_t w0,
+                                         uint64_t w1) {
+  if (ok && (single || (c >= w0 && c < w1))) {
+    const uint32_t d = (uint32_t)(c - w0);
+    const unsigned long long m = 1ull << (d & 63);
+    if (!(bits[d >> 6] & m)) atomicOr(&bits[d >> 6], m);
   }
 }
 
@@ -656,8 +671,9 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     for (uint64_t w0 = rlo; w0 <= rhi; w0 += kBitmapBits) {
       const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
       const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
+      const bool single = w0 == rlo && rhi < w0 + kBitmapBits;
       block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, [&](uint32_t c, double, bool ok) {
-        warp_mark_bit(S.bits, c, ok, w0, w1);
+        mark_bit(S.bits, c, ok, single, w0, w1);
       });
       unsigned long long cnt = 0;
       for (uint32_t w = tid; w < nwords; w += kBitmapThreads) {
@@ -717,7 +733,8 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
       const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
       // pass 1: mark columns
-      auto mark = [&](uint32_t c, double, bool ok) { warp_mark_bit(S.bits, c, ok, w0, w1); };
+      const bool single = w0 == rlo && rhi < w0 + kBitmapBits;
+      auto mark = [&](uint32_t c, double, bool ok) { mark_bit(S.bits, c, ok, single, w0, w1); };
       if (one_chunk) block_run_chunk<kBitmapThreads, false>(B, S.e, mark);
       else block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, mark);
       // rank table: thread t owns words [16t, 16t+16)
@@ -757,7 +774,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       __syncthreads();
       // pass 2: accumulate values at their ranks
       auto accumulate = [&](uint32_t c, double v, bool ok) {
-        if (ok && c >= w0 && c < w1) {
+        if (ok && (single || (c >= w0 && c < w1))) {
           const uint32_t d = (uint32_t)(c - w0);
           const uint32_t w = d >> 6;
           const uint32_t r = S.spre[w >> 10] + S.wpre[w] + __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));

@@ -23,7 +23,7 @@ from typing import Any, Optional, Union
 import numpy as np
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "libocean.so"
+LIB_PATH = Path(os.environ.get("OCEAN_LIB", str(_PKG / "libocean.so")))
 
 OCEAN_OK = 0
 STATUS_NAMES = {0: "OK", 1: "CUDA", 2: "CAPACITY", 3: "TIMEOUT", 4: "INVALID", 5: "OOM", 6: "INTERNAL"}
