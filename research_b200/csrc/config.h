@@ -186,6 +186,7 @@ struct Config {
   int force_sym_bin = -1;         // testing: put every non-empty row in one symbolic class
   int force_num_bin = -1;         // testing: put every non-empty row in one numeric class
   bool sync_on_return = true;     // check device status before returning
+  double bitmap_cache_fraction = 0.25;  // share of free device memory the saved row bitmaps may use
 
   static Config from_json_text(const std::string& text) {
     Config c;
@@ -246,8 +247,11 @@ struct Config {
     geti("force_sym_bin", c.force_sym_bin);
     geti("force_num_bin", c.force_num_bin);
     getb("sync_on_return", c.sync_on_return);
+    getd("bitmap_cache_fraction", c.bitmap_cache_fraction);
     if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
+    if (c.bitmap_cache_fraction < 0.0 || c.bitmap_cache_fraction > 0.9)
+      throw std::invalid_argument("bitmap_cache_fraction must be in [0, 0.9]");
     if (c.esc_max_products < 0 || c.esc_max_products > 32)
       throw std::invalid_argument("esc_max_products must be in [0, 32]");
     return c;

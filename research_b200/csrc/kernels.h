@@ -19,6 +19,9 @@ struct DevWork {
   unsigned long long* tile_sums = nullptr;
   uint64_t* rowptr64 = nullptr;  // rows+1 exclusive scan of row_nnz
   uint32_t* rowptr32 = nullptr;  // same, truncated to 32 bits
+  uint64_t* bm_off = nullptr;    // per row: word offset of its cached bitmap, or ~0
+  unsigned long long* bm_cache = nullptr;  // exact column bitmaps saved by the symbolic pass
+  uint64_t bm_cache_words = 0;   // capacity of bm_cache (0: no cache)
   DevCounters* ctr = nullptr;
 };
 

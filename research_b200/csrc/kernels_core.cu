@@ -112,13 +112,15 @@ template <typename RP, int G>
 __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
                                                   uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
                                                   uint32_t* __restrict__ anz, uint32_t* __restrict__ row_nnz,
+                                                  uint64_t* __restrict__ bm_off,
                                                   uint32_t* __restrict__ sym_bins,
                                                   DevCounters* __restrict__ ctr, SymPolicy pol) {
-  __shared__ unsigned long long s_anz[SB_COUNT], s_prod[SB_COUNT];
+  __shared__ unsigned long long s_anz[SB_COUNT], s_prod[SB_COUNT], s_words;
   if (threadIdx.x < SB_COUNT) {
     s_anz[threadIdx.x] = 0ull;
     s_prod[threadIdx.x] = 0ull;
   }
+  if (threadIdx.x == 0) s_words = 0ull;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int sl = lane & (G - 1);
@@ -153,12 +155,15 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     lo[row] = mn;
     hi[row] = mx;
     anz[row] = (uint32_t)(a1 - a0);
+    bm_off[row] = ~0ull;
     if (p == 0) {
       row_nnz[row] = 0;
     } else {
-      b = sym_bin_for(p, (uint64_t)mx - mn + 1, pol);
+      const uint64_t span = (uint64_t)mx - mn + 1;
+      b = sym_bin_for(p, span, pol);
       atomicAdd(&s_anz[b], (unsigned long long)(a1 - a0));
       atomicAdd(&s_prod[b], p);
+      if (b == SB_BITMAP && span <= kBitmapBits) atomicAdd(&s_words, (unsigned long long)((span + 63) >> 6));
     }
   }
   bin_append(b, (uint32_t)row, ctr->sym_count, sym_bins, A.rows);
@@ -179,6 +184,7 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     if (s_anz[threadIdx.x]) atomicAdd(&ctr->sym_anz[threadIdx.x], s_anz[threadIdx.x]);
     if (s_prod[threadIdx.x]) atomicAdd(&ctr->sym_prod[threadIdx.x], s_prod[threadIdx.x]);
   }
+  if (threadIdx.x == 0 && s_words) atomicAdd(&ctr->sym_words, s_words);
 }
 
 // ---------------------------------------------------------------- ESC (<= 32 products)
@@ -645,6 +651,7 @@ struct BitmapSymSmem {
   unsigned long long bits[kBitmapWords];
   EnumSmem<kBitmapThreads> e;
   unsigned long long red[33];
+  unsigned long long slot;
   uint32_t s_idx;
 };
 
@@ -652,7 +659,8 @@ template <typename RP>
 __global__ void __launch_bounds__(kBitmapThreads, 1)
     k_sym_bitmap(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins, DevCounters* __restrict__ ctr,
                  const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
-                 const uint32_t* __restrict__ hi, uint32_t* __restrict__ row_nnz) {
+                 const uint32_t* __restrict__ hi, uint32_t* __restrict__ row_nnz, uint64_t* __restrict__ bm_off,
+                 unsigned long long* __restrict__ cache, uint64_t cache_words) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BitmapSymSmem& S = *reinterpret_cast<BitmapSymSmem*>(smem_raw);
   const int tid = threadIdx.x;
@@ -675,9 +683,23 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, [&](uint32_t c, double, bool ok) {
         mark_bit(S.bits, c, ok, single, w0, w1);
       });
+      // a single-window row's exact bitmap is saved for the numeric pass when room is left
+      if (tid == 0) {
+        unsigned long long slot = ~0ull;
+        if (single && cache_words) {
+          const unsigned long long at = atomicAdd(&ctr->cache_cursor, (unsigned long long)nwords);
+          if (at + nwords <= cache_words) slot = at;
+        }
+        S.slot = slot;
+        if (single) bm_off[row] = slot;
+      }
+      __syncthreads();
+      const unsigned long long slot = S.slot;
       unsigned long long cnt = 0;
       for (uint32_t w = tid; w < nwords; w += kBitmapThreads) {
-        cnt += __popcll(S.bits[w]);
+        const unsigned long long word = S.bits[w];
+        cnt += __popcll(word);
+        if (slot != ~0ull) cache[slot + w] = word;
         S.bits[w] = 0ull;
       }
       total += block_sum_u64<kBitmapThreads>(cnt, S.red);
@@ -686,16 +708,15 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
   }
 }
 
-// Numeric: bitmap-rank accumulator. Pass 1 marks the output columns of the
-// window; a block scan turns the bitmap into a rank table (u16 word offsets
-// inside 1024-word superblocks plus u32 superblock offsets); the sorted column
-// ids are written from the bitmap and the values are accumulated straight into
-// C at position rank(column) with FP64 reductions in L2. Output is sorted by
-// construction; no hash collisions, no sort.
+// Numeric: bitmap-rank accumulator. The row's output columns are marked in a
+// bitmap (pass 1, or reloaded from the copy the symbolic pass saved); a block
+// scan turns it into a rank table (exclusive popcount of every 64-bit word);
+// the sorted column ids are written from the bitmap, and the values are
+// accumulated straight into C at position rank(column) with FP64 reductions in
+// L2 (pass 2). Output is sorted by construction: no hash collisions, no sort.
 struct BitmapNumSmem {
   unsigned long long bits[kBitmapWords];
-  uint16_t wpre[kBitmapWords];
-  uint32_t spre[kSupers];
+  uint32_t wpre[kBitmapWords];  // exclusive popcount of the words before each word
   uint32_t scan[33];
   EnumSmem<kBitmapThreads> e;
   uint32_t s_idx;
@@ -706,11 +727,12 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     k_num_bitmap(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins, DevCounters* __restrict__ ctr,
                  const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
                  const uint32_t* __restrict__ hi, const uint32_t* __restrict__ row_nnz,
-                 const uint64_t* __restrict__ rowptr, uint32_t* __restrict__ c_col,
+                 const uint64_t* __restrict__ rowptr, const uint64_t* __restrict__ bm_off,
+                 const unsigned long long* __restrict__ cache, uint32_t* __restrict__ c_col,
                  double* __restrict__ c_val) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BitmapNumSmem& S = *reinterpret_cast<BitmapNumSmem*>(smem_raw);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int i = tid; i < kBitmapWords; i += kBitmapThreads) S.bits[i] = 0ull;
   const uint32_t count = ctr->num_count[NB_BITMAP];
   const uint32_t* list = bins + (uint64_t)NB_BITMAP * A.rows;
@@ -725,6 +747,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     const uint64_t row_off = rowptr[row];
     const uint32_t expect = row_nnz[row];
     const uint64_t row_lim = row_off + expect;
+    const uint64_t slot = cache ? bm_off[row] : ~0ull;
     uint64_t off = row_off;
     // a row whose A entries fit one chunk is loaded once for both passes
     const bool one_chunk = a1 - a0 <= (uint64_t)kBitmapThreads;
@@ -732,12 +755,18 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     for (uint64_t w0 = rlo; w0 <= rhi; w0 += kBitmapBits) {
       const uint64_t w1 = min(rhi + 1, w0 + kBitmapBits);
       const uint32_t nwords = (uint32_t)((w1 - w0 + 63) >> 6);
-      // pass 1: mark columns
       const bool single = w0 == rlo && rhi < w0 + kBitmapBits;
-      auto mark = [&](uint32_t c, double, bool ok) { mark_bit(S.bits, c, ok, single, w0, w1); };
-      if (one_chunk) block_run_chunk<kBitmapThreads, false>(B, S.e, mark);
-      else block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, mark);
-      // rank table: thread t owns words [16t, 16t+16)
+      if (single && slot != ~0ull) {
+        // reload the exact bitmap saved by the symbolic pass
+        for (uint32_t w = tid; w < nwords; w += kBitmapThreads) S.bits[w] = cache[slot + w];
+        __syncthreads();
+      } else {
+        // pass 1: mark columns
+        auto mark = [&](uint32_t c, double, bool ok) { mark_bit(S.bits, c, ok, single, w0, w1); };
+        if (one_chunk) block_run_chunk<kBitmapThreads, false>(B, S.e, mark);
+        else block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, mark);
+      }
+      // rank table: thread t scans words [16t, 16t+16)
       const uint32_t wbeg = (uint32_t)tid * kWordsPerThread;
       uint32_t local = 0;
 #pragma unroll
@@ -746,30 +775,57 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
         local += (w < nwords) ? __popcll(S.bits[w]) : 0u;
       }
       uint32_t nw_total;
-      const uint32_t tpre = block_excl_scan<kBitmapThreads, uint32_t>(local, S.scan, &nw_total);
-      if ((tid & 63) == 0) S.spre[tid >> 6] = tpre;
-      __syncthreads();
-      {
-        const uint32_t sp = S.spre[tid >> 6];
-        uint32_t run = tpre;
-#pragma unroll 4
-        for (int i = 0; i < kWordsPerThread; ++i) {
-          const uint32_t w = wbeg + i;
-          if (w >= nwords) break;
-          unsigned long long word = S.bits[w];
-          S.wpre[w] = (uint16_t)(run - sp);
-          // sorted column ids of this word
-          while (word) {
-            const int bpos = __ffsll((long long)word) - 1;
-            word &= word - 1;
-            const uint64_t o = off + run;
-            if (o < row_lim) c_col[o] = (uint32_t)(w0 + (uint64_t)w * 64 + bpos);
-            ++run;
-          }
+      uint32_t run = block_excl_scan<kBitmapThreads, uint32_t>(local, S.scan, &nw_total);
+#pragma unroll
+      for (int i = 0; i < kWordsPerThread; ++i) {
+        const uint32_t w = wbeg + i;
+        if (w < nwords) {
+          S.wpre[w] = run;
+          run += __popcll(S.bits[w]);
         }
       }
-      for (uint32_t i = tid; i < nw_total; i += kBitmapThreads) {
-        if (off + i < row_lim) c_val[off + i] = 0.0;
+      __syncthreads();
+      // ordered output of the column ids (and zeroed values): warp w writes the
+      // words [512w, 512w + 512); sparse words one lane each, dense words
+      // (more than 8 bits) by the whole warp with coalesced stores
+      const uint32_t wend = min(nwords, (uint32_t)(warp + 1) * 512u);
+      for (uint32_t wb = (uint32_t)warp * 512u; wb < wend; wb += 32) {
+        const uint32_t w = wb + lane;
+        const unsigned long long word = w < wend ? S.bits[w] : 0ull;
+        const uint32_t pre = w < wend ? S.wpre[w] : 0u;
+        const bool dense = __popcll(word) > 8;
+        if (!dense) {
+          unsigned long long x = word;
+          uint32_t pos = pre;
+          while (x) {
+            const int bpos = __ffsll((long long)x) - 1;
+            x &= x - 1;
+            const uint64_t o = off + pos;
+            if (o < row_lim) {
+              c_col[o] = (uint32_t)(w0 + (uint64_t)w * 64 + bpos);
+              c_val[o] = 0.0;
+            }
+            ++pos;
+          }
+        }
+        unsigned dm = __ballot_sync(kFull, dense);
+        while (dm) {
+          const int src = __ffs(dm) - 1;
+          dm &= dm - 1;
+          const unsigned long long wv = __shfl_sync(kFull, word, src);
+          const uint32_t p0 = __shfl_sync(kFull, pre, src);
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int b = lane + 32 * h;
+            if ((wv >> b) & 1ull) {
+              const uint64_t o = off + p0 + __popcll(wv & ((1ull << b) - 1ull));
+              if (o < row_lim) {
+                c_col[o] = (uint32_t)(w0 + (uint64_t)(wb + src) * 64 + b);
+                c_val[o] = 0.0;
+              }
+            }
+          }
+        }
       }
       __syncthreads();
       // pass 2: accumulate values at their ranks
@@ -777,7 +833,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
         if (ok && (single || (c >= w0 && c < w1))) {
           const uint32_t d = (uint32_t)(c - w0);
           const uint32_t w = d >> 6;
-          const uint32_t r = S.spre[w >> 10] + S.wpre[w] + __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));
+          const uint32_t r = S.wpre[w] + __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));
           if (off + r < row_lim) atomicAdd(&c_val[off + r], v);
         }
       };
@@ -846,6 +902,7 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
                                                      const uint32_t* __restrict__ lo,
                                                      const uint32_t* __restrict__ hi,
                                                      const uint32_t* __restrict__ anz,
+                                                     const uint64_t* __restrict__ bm_off,
                                                      uint32_t* __restrict__ num_bins,
                                                      DevCounters* __restrict__ ctr, NumPolicy pol) {
   __shared__ unsigned long long scr[33];
@@ -875,6 +932,7 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
       run += v[q];
       const uint32_t p = prod[i];
       b = num_bin_for(v[q], p, (uint64_t)hi[i] - lo[i] + 1, pol);
+      if (b >= 0 && pol.force_bin < 0 && bm_off[i] != ~0ull) b = NB_BITMAP;  // reuse the saved bitmap
       if (b >= 0) {
         atomicAdd(&s_cls[b], (unsigned long long)v[q]);
         atomicAdd(&s_anz[b], (unsigned long long)anz[i]);
@@ -977,11 +1035,11 @@ void launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const
   if (avg >= 12.0) {
     const uint64_t threads = A.rows * 32;
     k_analysis<RP, 32><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.sym_bins, w.ctr, pol);
+        A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
   } else {
     const uint64_t threads = A.rows * 4;
     k_analysis<RP, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.sym_bins, w.ctr, pol);
+        A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
   }
 }
 
@@ -1005,7 +1063,7 @@ void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int n
       A, B, w.sym_bins, w.ctr, SB_HASH_L, w.prod, w.row_nnz);
   mark(4);
   k_sym_bitmap<RP><<<num_sms * g_occ[K_SYM_BM], kBitmapThreads, kSymBitmapSmem, s>>>(
-      A, B, w.sym_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz);
+      A, B, w.sym_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz, w.bm_off, w.bm_cache, w.bm_cache_words);
   mark(5);
 }
 
@@ -1015,7 +1073,7 @@ void launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s) {
   k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums);
   k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, w.ctr, w.rowptr64, w.rowptr32, w.rows);
   k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums, w.rowptr64, w.rowptr32,
-                                             w.prod, w.lo, w.hi, w.anz, w.num_bins, w.ctr, pol);
+                                             w.prod, w.lo, w.hi, w.anz, w.bm_off, w.num_bins, w.ctr, pol);
 }
 
 template <typename RP>
@@ -1039,7 +1097,7 @@ void launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32
       A, B, w.num_bins, w.ctr, NB_HASH_L, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
   mark(4);
   k_num_bitmap<RP><<<num_sms * g_occ[K_NUM_BM], kBitmapThreads, kNumBitmapSmem, s>>>(
-      A, B, w.num_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz, w.rowptr64, c_col, c_val);
+      A, B, w.num_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz, w.rowptr64, w.bm_off, w.bm_cache, c_col, c_val);
   mark(5);
 }
 

@@ -80,6 +80,8 @@ struct Stats {
   uint64_t num_prod[NB_COUNT] = {0};
   uint64_t sym_anz[SB_COUNT] = {0};
   uint64_t sym_prod[SB_COUNT] = {0};
+  uint64_t cache_words = 0, cache_used = 0;
+  bool cache_dropped = false;
   int workflow = 0;  // 0 = precise (symbolic + numeric)
   int rowptr_bits = 32;
   bool valid = false;
@@ -150,7 +152,7 @@ struct ocean_handle {
   void free_all() {
     DevWork& x = w;
     void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
-                  x.rowptr32, x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
+                  x.rowptr32, x.bm_off, x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
     for (void* p : ps)
       if (p) cudaFree(p);
     if (h_ctr) cudaFreeHost(h_ctr);
@@ -190,7 +192,8 @@ void ensure_rows(ocean_handle* h, uint64_t rows) {
     return;
   }
   DevWork& x = h->w;
-  void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32};
+  void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32,
+                x.bm_off};
   for (void* p : ps)
     if (p) cudaFree(p);
   const uint64_t r = std::max<uint64_t>(rows, 1);
@@ -204,6 +207,7 @@ void ensure_rows(ocean_handle* h, uint64_t rows) {
   OCEAN_CUDA(cudaMalloc((void**)&x.tile_sums, scan_tiles(r) * 8 + 8));
   OCEAN_CUDA(cudaMalloc((void**)&x.rowptr64, (r + 1) * 8));
   OCEAN_CUDA(cudaMalloc((void**)&x.rowptr32, (r + 1) * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.bm_off, r * 8));
   h->cap_rows = r;
   x.rows = rows;
 }
@@ -254,8 +258,28 @@ Csr<RP> to_csr(const ocean_csr_view* m, const RP* rp) {
 
 // Runs analysis + symbolic + scan. Leaves exact per-row counts in w.row_nnz,
 // row pointers in w.rowptr64/32 and the counters in h->h_ctr (read back).
+// Bytes the device could still hand out: free memory plus what the stream-ordered
+// pool holds in reserve.
+uint64_t available_device_bytes(int device) {
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  }
+  return (uint64_t)free_b + (reserved > used ? reserved - used : 0);
+}
+
+// Runs analysis + symbolic + scan. Leaves exact per-row counts in w.row_nnz,
+// row pointers in w.rowptr64/32 and the counters in h->h_ctr (read back).
+// With allow_cache, the symbolic pass saves the bitmaps of single-window
+// bitmap-class rows into h->w.bm_cache (allocated here on `s`, sized from the
+// analysis read-back and capped by bitmap_cache_fraction of free memory).
 template <typename RP>
-void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool with_scan) {
+void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool with_scan,
+               bool allow_cache) {
   ensure_rows(h, A.rows);
   OCEAN_CUDA(cudaMemsetAsync(h->w.ctr, 0, sizeof(DevCounters), s));
   SymPolicy sp;
@@ -265,10 +289,28 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   np.esc_max_products = (uint32_t)h->cfg.esc_max_products;
   np.force_bin = h->cfg.force_num_bin;
   OCEAN_CHECK(sp.force_bin < SB_COUNT && np.force_bin < NB_COUNT, OCEAN_ERR_INVALID, "forced class out of range");
+  h->w.bm_cache = nullptr;
+  h->w.bm_cache_words = 0;
   record(h, EV_START, s);
   launch_analysis(A, B, h->w, sp, s);
   OCEAN_CUDA(cudaGetLastError());
   record(h, EV_ANALYSIS, s);
+  if (allow_cache && h->cfg.bitmap_cache_fraction > 0.0) {
+    OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+    OCEAN_CUDA(cudaStreamSynchronize(s));
+    const uint64_t want = h->h_ctr->sym_words;
+    const uint64_t budget = (uint64_t)(h->cfg.bitmap_cache_fraction * (double)available_device_bytes(h->device)) / 8;
+    const uint64_t words = std::min(want, budget);
+    if (words >= 1024) {
+      void* p = nullptr;
+      if (cudaMallocAsync(&p, words * 8, s) == cudaSuccess) {
+        h->w.bm_cache = (unsigned long long*)p;
+        h->w.bm_cache_words = words;
+      } else {
+        cudaGetLastError();
+      }
+    }
+  }
   launch_symbolic(A, B, h->w, h->num_sms, s, h->ev + EV_SYM0);
   OCEAN_CUDA(cudaGetLastError());
   if (with_scan) {
@@ -279,6 +321,12 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
   OCEAN_CUDA(cudaStreamSynchronize(s));
   check_device_status(h);
+}
+
+void release_cache(ocean_handle* h, cudaStream_t s) {
+  if (h->w.bm_cache) cudaFreeAsync(h->w.bm_cache, s);
+  h->w.bm_cache = nullptr;
+  h->w.bm_cache_words = 0;
 }
 
 template <typename RP>
@@ -295,7 +343,12 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
 
   uint64_t nnz = 0;
   if (A.rows > 0) {
-    run_front(h, A, B, s, true);
+    try {
+      run_front(h, A, B, s, true, true);
+    } catch (...) {
+      release_cache(h, s);
+      throw;
+    }
     nnz = h->h_ctr->total_nnz;
   } else {
     std::memset(h->h_ctr, 0, sizeof(DevCounters));
@@ -303,11 +356,30 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   int bits = h->cfg.output_rowptr_bits ? h->cfg.output_rowptr_bits : (nnz >= (1ull << 32) ? 64 : 32);
   OCEAN_CHECK(!(bits == 32 && nnz >= (1ull << 32)), OCEAN_ERR_INVALID,
               "nnz(C) >= 2^32 does not fit 32-bit row pointers (output_rowptr_bits=32)");
+  st.cache_words = h->w.bm_cache_words;
+  st.cache_used = std::min<uint64_t>(h->h_ctr->cache_cursor, h->w.bm_cache_words);
   CResult* owner = new CResult{0};
   try {
-    OCEAN_CUDA(cudaMallocAsync(&owner->rowptr, (A.rows + 1) * (bits / 8), s));
-    OCEAN_CUDA(cudaMallocAsync((void**)&owner->col, std::max<uint64_t>(nnz, 1) * 4, s));
-    OCEAN_CUDA(cudaMallocAsync((void**)&owner->val, std::max<uint64_t>(nnz, 1) * 8, s));
+    // C is allocated after the saved bitmaps; if it does not fit, the bitmaps
+    // are dropped (the numeric pass then marks its columns itself) and C retried.
+    auto alloc_c = [&]() -> cudaError_t {
+      cudaError_t e = cudaMallocAsync(&owner->rowptr, (A.rows + 1) * (bits / 8), s);
+      if (e == cudaSuccess) e = cudaMallocAsync((void**)&owner->col, std::max<uint64_t>(nnz, 1) * 4, s);
+      if (e == cudaSuccess) e = cudaMallocAsync((void**)&owner->val, std::max<uint64_t>(nnz, 1) * 8, s);
+      return e;
+    };
+    cudaError_t e = alloc_c();
+    if (e != cudaSuccess && h->w.bm_cache) {
+      cudaGetLastError();
+      for (void** p : {&owner->rowptr, (void**)&owner->col, (void**)&owner->val}) {
+        if (*p) cudaFreeAsync(*p, s);
+        *p = nullptr;
+      }
+      release_cache(h, s);
+      st.cache_dropped = true;
+      e = alloc_c();
+    }
+    OCEAN_CUDA(e);
     if (A.rows > 0) {
       launch_numeric(A, B, h->w, owner->col, owner->val, h->num_sms, s, h->ev + EV_NUM0);
       OCEAN_CUDA(cudaGetLastError());
@@ -317,6 +389,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
       OCEAN_CUDA(cudaMemsetAsync(owner->rowptr, 0, bits / 8, s));
       for (int i = EV_START; i < EV_END; ++i) record(h, i, s);
     }
+    release_cache(h, s);
     record(h, EV_END, s);
     h->ev_recorded = true;
     h->tracked = h->cfg.track_stage_times;
@@ -326,6 +399,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
       check_device_status(h);
     }
   } catch (...) {
+    release_cache(h, s);
     if (owner->rowptr) cudaFreeAsync(owner->rowptr, s);
     if (owner->col) cudaFreeAsync(owner->col, s);
     if (owner->val) cudaFreeAsync(owner->val, s);
@@ -418,7 +492,9 @@ std::string stats_json(ocean_handle* h) {
     << ", \"intermediate_product_max\": " << st.max_products << ", \"intermediate_product_avg\": " << avg
     << ", \"input_expansion\": " << ie << ", \"output_compression\": " << oc
     << ", \"max_a_row_nnz\": " << st.max_a_nnz << "}, ";
-  o << "\"decision\": {\"workflow\": " << st.workflow << ", \"rowptr_bits\": " << st.rowptr_bits << "}, ";
+  o << "\"decision\": {\"workflow\": " << st.workflow << ", \"rowptr_bits\": " << st.rowptr_bits
+    << ", \"bitmap_cache_bytes\": " << 8 * st.cache_words << ", \"bitmap_cache_used_bytes\": " << 8 * st.cache_used
+    << ", \"bitmap_cache_dropped\": " << (st.cache_dropped ? "true" : "false") << "}, ";
   o << "\"binning_1\": [";
   for (int i = 0; i < SB_COUNT; ++i) o << (i ? ", " : "") << st.sym_bins[i];
   o << "], \"binning_2\": [";
@@ -650,10 +726,10 @@ int ocean_symbolic(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_vie
     cudaStream_t s = (cudaStream_t)stream;
     if (A->rowptr_bits == 32) {
       run_front(h, to_csr<uint32_t>(A, (const uint32_t*)A->rowptr), to_csr<uint32_t>(B, (const uint32_t*)B->rowptr),
-                s, false);
+                s, false, false);
     } else {
       run_front(h, to_csr<uint64_t>(A, (const uint64_t*)A->rowptr), to_csr<uint64_t>(B, (const uint64_t*)B->rowptr),
-                s, false);
+                s, false, false);
     }
     OCEAN_CUDA(cudaMemcpyAsync(row_nnz, h->w.row_nnz, A->rows * 4, cudaMemcpyDeviceToDevice, s));
     OCEAN_CUDA(cudaStreamSynchronize(s));

@@ -52,6 +52,8 @@ struct DevCounters {
   unsigned long long num_prod[NB_COUNT];  // products of the rows of each numeric class
   unsigned long long sym_anz[SB_COUNT];   // A entries of the rows of each symbolic class
   unsigned long long sym_prod[SB_COUNT];  // products of the rows of each symbolic class
+  unsigned long long sym_words;           // bitmap words of single-window bitmap-class rows
+  unsigned long long cache_cursor;        // words handed out from the bitmap cache
   unsigned int status;     // OR of DevError bits
   unsigned int err_row;
   unsigned int pad[4];

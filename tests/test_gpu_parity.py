@@ -214,3 +214,14 @@ def test_murmur3_device_matches_reference_kat(murmur_kat):
     keys, hashes = murmur_kat
     out = murmur3_device(torch.from_numpy(keys.view(np.int32)).cuda(), 1234)
     assert np.array_equal(out.cpu().numpy().view(np.uint32), hashes)
+
+
+@pytest.mark.parametrize("frac", [0.0, 0.25])
+def test_bitmap_cache_on_and_off(frac):
+    # rows of the bitmap class either reload the bitmap saved by the symbolic
+    # pass or mark their columns again; both must give the oracle's C
+    A = M.rmat(15, 16, seed=3)
+    C, st = multiply_device(A, A, {"bitmap_cache_fraction": frac})
+    check(A, A, C)
+    used = st["decision"]["bitmap_cache_used_bytes"]
+    assert (used > 0) == (frac > 0)
