@@ -58,6 +58,13 @@ def make_workload(name: str):
         p, _, _ = O.row_stats(A, A)
         rows = np.nonzero(p > 16384)[0][::64]
         return take_rows(A, rows), A, f"{rows.size} heavy rows of R-MAT n=2^20 (every 64th with >16384 products) times A"
+    if name == "rmat20m":
+        # profiling case: every 32nd heavy row with 16384 < products < 1e6 of the R-MAT 2^20 workload times A
+        from oracle import oracle as O
+        A = M.rmat(20, 16, (0.57, 0.19, 0.19, 0.05), seed=0)
+        p, _, _ = O.row_stats(A, A)
+        rows = np.nonzero((p > 16384) & (p < 1_000_000))[0][::32]
+        return take_rows(A, rows), A, f"{rows.size} typical heavy rows of R-MAT n=2^20 (every 32nd with 16384 < products < 1e6) times A"
     if name.startswith("rmat"):
         sc = int(name[4:])
         A = M.rmat(sc, 16, (0.57, 0.19, 0.19, 0.05), seed=0)

@@ -710,13 +710,15 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
 
 // Numeric: bitmap-rank accumulator. The row's output columns are marked in a
 // bitmap (pass 1, or reloaded from the copy the symbolic pass saved); a block
-// scan turns it into a rank table (exclusive popcount of every 64-bit word);
+// scan turns it into a rank table (u16 exclusive popcount of every 64-bit word
+// inside its 1024-word superblock plus u32 superblock offsets);
 // the sorted column ids are written from the bitmap, and the values are
 // accumulated straight into C at position rank(column) with FP64 reductions in
 // L2 (pass 2). Output is sorted by construction: no hash collisions, no sort.
 struct BitmapNumSmem {
   unsigned long long bits[kBitmapWords];
-  uint32_t wpre[kBitmapWords];  // exclusive popcount of the words before each word
+  uint16_t wpre[kBitmapWords];        // popcount of the words before each word, within its 1024-word superblock
+  uint32_t spre[kBitmapWords / 1024];  // popcount of the superblocks before each superblock
   uint32_t scan[33];
   EnumSmem<kBitmapThreads> e;
   uint32_t s_idx;
@@ -776,23 +778,26 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       }
       uint32_t nw_total;
       uint32_t run = block_excl_scan<kBitmapThreads, uint32_t>(local, S.scan, &nw_total);
+      if ((tid & 63) == 0) S.spre[tid >> 6] = run;
+      __syncthreads();
+      const uint32_t sp0 = S.spre[tid >> 6];
 #pragma unroll
       for (int i = 0; i < kWordsPerThread; ++i) {
         const uint32_t w = wbeg + i;
         if (w < nwords) {
-          S.wpre[w] = run;
+          S.wpre[w] = (uint16_t)(run - sp0);
           run += __popcll(S.bits[w]);
         }
       }
       __syncthreads();
-      // ordered output of the column ids (and zeroed values): warp w writes the
-      // words [512w, 512w + 512); sparse words one lane each, dense words
-      // (more than 8 bits) by the whole warp with coalesced stores
-      const uint32_t wend = min(nwords, (uint32_t)(warp + 1) * 512u);
-      for (uint32_t wb = (uint32_t)warp * 512u; wb < wend; wb += 32) {
+      // ordered output of the column ids (and zeroed values): 32-word groups go
+      // to the warps round-robin (dense low-index regions spread over all
+      // warps); sparse words are written by one lane each, dense words (more
+      // than 8 bits) by the whole warp with coalesced stores
+      for (uint32_t wb = (uint32_t)warp * 32u; wb < nwords; wb += 32u * (kBitmapThreads / 32)) {
         const uint32_t w = wb + lane;
-        const unsigned long long word = w < wend ? S.bits[w] : 0ull;
-        const uint32_t pre = w < wend ? S.wpre[w] : 0u;
+        const unsigned long long word = w < nwords ? S.bits[w] : 0ull;
+        const uint32_t pre = w < nwords ? S.spre[w >> 10] + S.wpre[w] : 0u;
         const bool dense = __popcll(word) > 8;
         if (!dense) {
           unsigned long long x = word;
@@ -833,7 +838,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
         if (ok && (single || (c >= w0 && c < w1))) {
           const uint32_t d = (uint32_t)(c - w0);
           const uint32_t w = d >> 6;
-          const uint32_t r = S.wpre[w] + __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));
+          const uint32_t r = S.spre[w >> 10] + S.wpre[w] + __popcll(S.bits[w] & ((1ull << (d & 63)) - 1ull));
           if (off + r < row_lim) atomicAdd(&c_val[off + r], v);
         }
       };

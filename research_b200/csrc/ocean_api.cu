@@ -148,6 +148,9 @@ struct ocean_handle {
   double* out_val = nullptr;
   uint64_t out_val_cap = 0;
   CResult host_owner{1};
+  // saved row bitmaps of the symbolic pass (grow-only, kept across calls)
+  unsigned long long* cache_buf = nullptr;
+  uint64_t cache_cap_words = 0;
 
   void free_all() {
     DevWork& x = w;
@@ -159,6 +162,7 @@ struct ocean_handle {
     if (out_rp) cudaFreeHost(out_rp);
     if (out_col) cudaFreeHost(out_col);
     if (out_val) cudaFreeHost(out_val);
+    if (cache_buf) cudaFree(cache_buf);
     for (auto& e : ev) cudaEventDestroy(e);
   }
 };
@@ -302,12 +306,20 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
     const uint64_t budget = (uint64_t)(h->cfg.bitmap_cache_fraction * (double)available_device_bytes(h->device)) / 8;
     const uint64_t words = std::min(want, budget);
     if (words >= 1024) {
-      void* p = nullptr;
-      if (cudaMallocAsync(&p, words * 8, s) == cudaSuccess) {
-        h->w.bm_cache = (unsigned long long*)p;
-        h->w.bm_cache_words = words;
-      } else {
-        cudaGetLastError();
+      if (h->cache_cap_words < words) {
+        if (h->cache_buf) cudaFree(h->cache_buf);
+        h->cache_buf = nullptr;
+        h->cache_cap_words = 0;
+        const uint64_t grow_to = std::min(budget, words + words / 8);
+        if (cudaMalloc((void**)&h->cache_buf, grow_to * 8) == cudaSuccess) {
+          h->cache_cap_words = grow_to;
+        } else {
+          cudaGetLastError();
+        }
+      }
+      if (h->cache_buf) {
+        h->w.bm_cache = h->cache_buf;
+        h->w.bm_cache_words = std::min(words, h->cache_cap_words);
       }
     }
   }
@@ -323,10 +335,21 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   check_device_status(h);
 }
 
-void release_cache(ocean_handle* h, cudaStream_t s) {
-  if (h->w.bm_cache) cudaFreeAsync(h->w.bm_cache, s);
+// Stops using the saved bitmaps for this call (the buffer stays with the handle).
+void release_cache(ocean_handle* h, cudaStream_t) {
   h->w.bm_cache = nullptr;
   h->w.bm_cache_words = 0;
+}
+
+// Frees the saved-bitmap buffer (when C needs the memory).
+void drop_cache_buffer(ocean_handle* h, cudaStream_t s) {
+  release_cache(h, s);
+  if (h->cache_buf) {
+    cudaStreamSynchronize(s);
+    cudaFree(h->cache_buf);
+  }
+  h->cache_buf = nullptr;
+  h->cache_cap_words = 0;
 }
 
 template <typename RP>
@@ -375,7 +398,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         if (*p) cudaFreeAsync(*p, s);
         *p = nullptr;
       }
-      release_cache(h, s);
+      drop_cache_buffer(h, s);
       st.cache_dropped = true;
       e = alloc_c();
     }
