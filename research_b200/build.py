@@ -70,13 +70,14 @@ def build_library(force: bool = False, verbose_ptxas: bool = False) -> Path:
 
 def build_cli(force: bool = False) -> Path:
     src = CSRC / "spgemm_main.cpp"
-    deps = [src, INCLUDE / "ocean.h", INCLUDE / "ocean_spgemm.hpp", LIB]
+    deps = [src, INCLUDE / "ocean.h", INCLUDE / "ocean_spgemm.hpp", CSRC / "config.h", LIB]
     if not src.exists():
         return CLI
     if not force and not _stale(CLI, deps):
         return CLI
     CLI.parent.mkdir(exist_ok=True)
-    _run(["g++", "-O2", "-std=c++17", "-I", str(INCLUDE), "-I", "/usr/local/cuda/include", str(src),
+    _run(["/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++", "-O2", "-std=c++17", "-I", str(INCLUDE),
+          "-I", str(CSRC), "-I", "/usr/local/cuda/include", str(src),
           "-o", str(CLI), "-L", str(PKG), "-locean", "-Wl,-rpath,$ORIGIN/..",
           "-L", "/usr/local/cuda/lib64", "-lcudart"])
     return CLI
