@@ -182,7 +182,7 @@ struct Config {
   int hll_higher_precision_expansion_threshold = 48;
   // this library's keys
   int output_rowptr_bits = 0;     // 0: 32 when nnz(C) < 2^32, else 64
-  int esc_max_products = 32;      // rows with at most this many products use the ESC class
+  int esc_max_products = 128;     // rows with at most this many products use the register ESC classes
   int force_sym_bin = -1;         // testing: put every non-empty row in one symbolic class
   int force_num_bin = -1;         // testing: put every non-empty row in one numeric class
   bool sync_on_return = true;     // check device status before returning
@@ -252,8 +252,8 @@ struct Config {
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
     if (c.bitmap_cache_fraction < 0.0 || c.bitmap_cache_fraction > 0.9)
       throw std::invalid_argument("bitmap_cache_fraction must be in [0, 0.9]");
-    if (c.esc_max_products < 0 || c.esc_max_products > 32)
-      throw std::invalid_argument("esc_max_products must be in [0, 32]");
+    if (c.esc_max_products < 0 || c.esc_max_products > 128)
+      throw std::invalid_argument("esc_max_products must be in [0, 128]");
     return c;
   }
 };

@@ -29,28 +29,32 @@ constexpr int kScanTile = 4096;
 inline uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
 
 struct SymPolicy {
-  uint32_t esc_max_products = 32;
+  uint32_t esc_max_products = 128;
   int force_bin = -1;   // >= 0: every non-empty row goes to this class (tests)
 };
 struct NumPolicy {
-  uint32_t esc_max_products = 32;
+  uint32_t esc_max_products = 128;
   int force_bin = -1;
 };
 
 template <typename RP>
-void launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
+int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
                      cudaStream_t s);
 
 // bin_events (optional): SB_COUNT + 1 events recorded around the class kernels.
+// counts (optional): host copy of the rows per class; empty classes are not
+// launched and grids are capped by the class size.
+// Each launcher returns the number of kernels it launched.
 template <typename RP>
-void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms,
-                     cudaStream_t s, cudaEvent_t* bin_events);
+int launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms,
+                    cudaStream_t s, cudaEvent_t* bin_events, const unsigned* counts = nullptr);
 
-void launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s);
+int launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s);
 
 template <typename RP>
-void launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_t* c_col,
-                    double* c_val, int num_sms, cudaStream_t s, cudaEvent_t* bin_events);
+int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_t* c_col,
+                    double* c_val, int num_sms, cudaStream_t s, cudaEvent_t* bin_events,
+                    const unsigned* counts = nullptr);
 
 void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, cudaStream_t s);
 

@@ -83,7 +83,7 @@ __device__ __forceinline__ void raise_status(DevCounters* ctr, unsigned bit, uin
 // Symbolic class of a row from its product count and output column span.
 __device__ __forceinline__ int sym_bin_for(uint64_t p, uint64_t span, const SymPolicy& pol) {
   if (pol.force_bin >= 0) return pol.force_bin;
-  if (p <= pol.esc_max_products) return SB_ESC;
+  if (p <= pol.esc_max_products) return p <= 32 ? SB_ESC1 : (p <= 64 ? SB_ESC2 : SB_ESC4);
   const uint64_t words = (span + 63) >> 6;
   if (p > 16384) return SB_BITMAP;
   if (p <= 1024) return SB_HASH_S;
@@ -96,7 +96,7 @@ __device__ __forceinline__ int num_bin_for(uint32_t n, uint64_t p, uint64_t span
                                            const NumPolicy& pol) {
   if (n == 0) return -1;
   if (pol.force_bin >= 0) return pol.force_bin;
-  if (p <= pol.esc_max_products) return NB_ESC;
+  if (p <= pol.esc_max_products) return p <= 32 ? NB_ESC1 : (p <= 64 ? NB_ESC2 : NB_ESC4);
   const uint64_t words = (span + 63) >> 6;
   if (n <= 512) return NB_HASH_S;
   if (n <= 2048) return (words <= 1024) ? NB_BITMAP : NB_HASH_M;
@@ -187,16 +187,24 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
   if (threadIdx.x == 0 && s_words) atomicAdd(&ctr->sym_words, s_words);
 }
 
-// ---------------------------------------------------------------- ESC (<= 32 products)
-// Lists the (<= 32) products of `row` in warp order: src[i] = index into B,
-// aidx[i] = index into A. Returns the product count.
-template <typename RP>
+// ---------------------------------------------------------------- ESC (<= 32K products)
+// Expand-sort-compress in the registers of one warp: a row's (<= 32K)
+// products are listed, held K per lane (element i = e*32 + lane lives in
+// register e of lane i%32), bitonic-sorted by column across the warp (shuffles
+// for partners in other lanes, register swaps for partners in the same lane),
+// then equal columns are merged by a segmented suffix sum that carries across
+// register rows. The output is the row, sorted, with no shared-memory table and
+// no block barrier. The symbolic variant sorts keys only and counts run heads.
+
+// Lists the (<= CAP) products of `row` in warp order: src[i] = index into B,
+// aidx[i] = index into A. Returns the product count (> CAP means overflow).
+template <int CAP, typename RP>
 __device__ __forceinline__ uint32_t gather_products(const Csr<RP>& A, const Csr<RP>& B, uint32_t row,
                                                     uint64_t* src, uint64_t* aidx) {
   const int lane = threadIdx.x & 31;
   const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
   uint32_t base = 0;
-  for (uint64_t k0 = a0; k0 < a1; k0 += 32) {
+  for (uint64_t k0 = a0; k0 < a1 && base <= CAP; k0 += 32) {
     const uint64_t k = k0 + lane;
     uint64_t b0 = 0;
     uint32_t len = 0;
@@ -204,7 +212,7 @@ __device__ __forceinline__ uint32_t gather_products(const Csr<RP>& A, const Csr<
       const uint32_t j = A.col[k];
       b0 = B.row_begin(j);
       const uint64_t l = B.row_end(j) - b0;
-      len = l > 64 ? 64u : (uint32_t)l;
+      len = l > CAP + 1 ? CAP + 1u : (uint32_t)l;
     }
     uint32_t incl = len;
 #pragma unroll
@@ -213,7 +221,7 @@ __device__ __forceinline__ uint32_t gather_products(const Csr<RP>& A, const Csr<
       if (lane >= o) incl += y;
     }
     const uint32_t excl = base + incl - len;
-    for (uint32_t t = 0; t < len && excl + t < 32; ++t) {
+    for (uint32_t t = 0; t < len && excl + t < CAP; ++t) {
       src[excl + t] = b0 + t;
       if (aidx) aidx[excl + t] = k;
     }
@@ -223,85 +231,178 @@ __device__ __forceinline__ uint32_t gather_products(const Csr<RP>& A, const Csr<
   return base;
 }
 
-template <typename RP>
+// Bitonic sort of the warp's 32K (key, value) elements, ascending by key.
+template <int K, bool VALS>
+__device__ __forceinline__ void warp_bitonic_sort(uint32_t (&key)[K], double (&val)[K]) {
+  const int lane = threadIdx.x & 31;
+  constexpr int N = 32 * K;
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const int je = j >> 5;
+#pragma unroll
+        for (int e = 0; e < K; ++e) {
+          if ((e & je) == 0) {
+            const int e2 = e | je;
+            const bool asc = (((e << 5) | lane) & k) == 0;
+            if ((key[e] > key[e2]) == asc) {
+              const uint32_t tk = key[e];
+              key[e] = key[e2];
+              key[e2] = tk;
+              if (VALS) {
+                const double tv = val[e];
+                val[e] = val[e2];
+                val[e2] = tv;
+              }
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < K; ++e) {
+          const uint32_t ok = __shfl_xor_sync(kFull, key[e], j);
+          double ov = 0.0;
+          if (VALS) ov = __shfl_xor_sync(kFull, val[e], j);
+          const bool asc = (((e << 5) | lane) & k) == 0;
+          const bool low = (lane & j) == 0;
+          const bool take = (low == asc) ? (ok < key[e]) : (ok > key[e]);
+          if (take) {
+            key[e] = ok;
+            if (VALS) val[e] = ov;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Run heads of the sorted keys: head if the key is real and differs from the
+// previous element in sort order. hb[e] = ballot of heads in register row e.
+template <int K>
+__device__ __forceinline__ void warp_run_heads(const uint32_t (&key)[K], unsigned (&hb)[K], bool (&head)[K]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int e = 0; e < K; ++e) {
+    const uint32_t up = __shfl_up_sync(kFull, key[e], 1);
+    uint32_t prev_last = kEmpty;
+    if (e > 0) prev_last = __shfl_sync(kFull, key[e - 1], 31);
+    const uint32_t prev = lane > 0 ? up : prev_last;
+    head[e] = key[e] != kEmpty && (((e << 5) | lane) == 0 || prev != key[e]);
+    hb[e] = __ballot_sync(kFull, head[e]);
+  }
+}
+
+template <typename RP, int K>
 __global__ void __launch_bounds__(256) k_sym_esc(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
-                                                 DevCounters* __restrict__ ctr,
+                                                 DevCounters* __restrict__ ctr, int bin,
                                                  uint32_t* __restrict__ row_nnz) {
-  __shared__ uint64_t s_src[8][32];
+  constexpr int CAP = 32 * K;
+  __shared__ uint64_t s_src[8][CAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t count = ctr->sym_count[SB_ESC];
-  const uint32_t* list = bins + (uint64_t)SB_ESC * A.rows;
+  const uint32_t count = ctr->sym_count[bin];
+  const uint32_t* list = bins + (uint64_t)bin * A.rows;
   for (uint64_t idx = (uint64_t)blockIdx.x * 8 + warp; idx < count; idx += (uint64_t)gridDim.x * 8) {
     const uint32_t row = list[idx];
-    const uint32_t np = gather_products(A, B, row, s_src[warp], nullptr);
-    if (np > 32 && lane == 0) raise_status(ctr, DEV_BIN_OVERFLOW, row);
-    const uint32_t col = lane < np ? B.col[s_src[warp][lane]] : kEmpty;
-    const unsigned peers = __match_any_sync(kFull, col);
-    const bool first = (col != kEmpty) && (__ffs(peers) - 1 == lane);
-    const unsigned n = __popc(__ballot_sync(kFull, first));
+    const uint32_t np = gather_products<CAP>(A, B, row, s_src[warp], nullptr);
+    if (np > CAP && lane == 0) raise_status(ctr, DEV_BIN_OVERFLOW, row);
+    uint32_t key[K];
+    double val[K];
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+      const uint32_t i = (uint32_t)(e << 5) | lane;
+      key[e] = i < np && i < (uint32_t)CAP ? B.col[s_src[warp][i]] : kEmpty;
+      val[e] = 0.0;
+    }
+    uint32_t n;
+    if (K == 1) {
+      // one product per lane: distinct count without sorting
+      const unsigned peers = __match_any_sync(kFull, key[0]);
+      const bool first = key[0] != kEmpty && (__ffs(peers) - 1 == lane);
+      n = __popc(__ballot_sync(kFull, first));
+    } else {
+      warp_bitonic_sort<K, false>(key, val);
+      unsigned hb[K];
+      bool head[K];
+      warp_run_heads<K>(key, hb, head);
+      n = 0;
+#pragma unroll
+      for (int e = 0; e < K; ++e) n += __popc(hb[e]);
+    }
     if (lane == 0) row_nnz[row] = n;
     __syncwarp();
   }
 }
 
-// Numeric ESC: one product per lane, 32-lane bitonic sort by column in
-// registers, segmented suffix sum, ordered write of the distinct columns.
-template <typename RP>
+template <typename RP, int K>
 __global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
-                                                 DevCounters* __restrict__ ctr,
+                                                 DevCounters* __restrict__ ctr, int bin,
                                                  const uint32_t* __restrict__ row_nnz,
                                                  const uint64_t* __restrict__ rowptr,
                                                  uint32_t* __restrict__ c_col, double* __restrict__ c_val) {
-  __shared__ uint64_t s_src[8][32];
-  __shared__ uint64_t s_aidx[8][32];
+  constexpr int CAP = 32 * K;
+  __shared__ uint64_t s_src[8][CAP];
+  __shared__ uint64_t s_aidx[8][CAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t count = ctr->num_count[NB_ESC];
-  const uint32_t* list = bins + (uint64_t)NB_ESC * A.rows;
+  const uint32_t count = ctr->num_count[bin];
+  const uint32_t* list = bins + (uint64_t)bin * A.rows;
   for (uint64_t idx = (uint64_t)blockIdx.x * 8 + warp; idx < count; idx += (uint64_t)gridDim.x * 8) {
     const uint32_t row = list[idx];
-    const uint32_t np = gather_products(A, B, row, s_src[warp], s_aidx[warp]);
-    if (np > 32 && lane == 0) raise_status(ctr, DEV_BIN_OVERFLOW, row);
-    uint32_t key = kEmpty;
-    double v = 0.0;
-    if (lane < np) {
-      const uint64_t s = s_src[warp][lane];
-      key = B.col[s];
-      v = A.val[s_aidx[warp][lane]] * B.val[s];
-    }
-    // bitonic sort of 32 (key, value) pairs across lanes, ascending
+    const uint32_t np = gather_products<CAP>(A, B, row, s_src[warp], s_aidx[warp]);
+    if (np > CAP && lane == 0) raise_status(ctr, DEV_BIN_OVERFLOW, row);
+    uint32_t key[K];
+    double val[K];
 #pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        const uint32_t ok = __shfl_xor_sync(kFull, key, j);
-        const double ov = __shfl_xor_sync(kFull, v, j);
-        const bool asc = (lane & k) == 0;
-        const bool low = (lane & j) == 0;
-        const bool take = (low == asc) ? (ok < key) : (ok > key);
-        if (take) {
-          key = ok;
-          v = ov;
-        }
+    for (int e = 0; e < K; ++e) {
+      const uint32_t i = (uint32_t)(e << 5) | lane;
+      key[e] = kEmpty;
+      val[e] = 0.0;
+      if (i < np && i < (uint32_t)CAP) {
+        const uint64_t sidx = s_src[warp][i];
+        key[e] = B.col[sidx];
+        val[e] = A.val[s_aidx[warp][i]] * B.val[sidx];
       }
     }
-    // segmented suffix sum: lanes holding the same column are adjacent
+    warp_bitonic_sort<K, true>(key, val);
+    // segmented suffix sums inside each register row
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t ck = __shfl_down_sync(kFull, key, d);
-      const double cv = __shfl_down_sync(kFull, v, d);
-      if (lane + d < 32 && ck == key) v += cv;
+    for (int e = 0; e < K; ++e) {
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t ck = __shfl_down_sync(kFull, key[e], d);
+        const double cv = __shfl_down_sync(kFull, val[e], d);
+        if (lane + d < 32 && ck == key[e]) val[e] += cv;
+      }
     }
-    const uint32_t prev = __shfl_up_sync(kFull, key, 1);
-    const bool head = key != kEmpty && (lane == 0 || prev != key);
-    const unsigned heads = __ballot_sync(kFull, head);
-    const uint32_t n = __popc(heads);
+    // carry runs that continue into the next register row, last row first
+    uint32_t carry_key = kEmpty;
+    double carry = 0.0;
+#pragma unroll
+    for (int e = K - 1; e >= 0; --e) {
+      const uint32_t last = __shfl_sync(kFull, key[e], 31);
+      if (key[e] == last && last == carry_key && last != kEmpty) val[e] += carry;
+      carry_key = __shfl_sync(kFull, key[e], 0);
+      carry = __shfl_sync(kFull, val[e], 0);
+    }
+    unsigned hb[K];
+    bool head[K];
+    warp_run_heads<K>(key, hb, head);
+    uint32_t n = 0;
+#pragma unroll
+    for (int e = 0; e < K; ++e) n += __popc(hb[e]);
     const uint32_t expect = row_nnz[row];
     if (n != expect && lane == 0) raise_status(ctr, DEV_COUNT_MISMATCH, row);
-    const uint32_t pos = __popc(heads & lanemask_lt());
-    if (head && pos < expect) {
-      const uint64_t off = rowptr[row] + pos;
-      c_col[off] = key;
-      c_val[off] = v;
+    const uint64_t off = rowptr[row];
+    uint32_t before = 0;
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+      const uint32_t pos = before + __popc(hb[e] & lanemask_lt());
+      if (head[e] && pos < expect) {
+        c_col[off + pos] = key[e];
+        c_val[off + pos] = val[e];
+      }
+      before += __popc(hb[e]);
     }
     __syncwarp();
   }
@@ -911,12 +1012,8 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
                                                      uint32_t* __restrict__ num_bins,
                                                      DevCounters* __restrict__ ctr, NumPolicy pol) {
   __shared__ unsigned long long scr[33];
-  __shared__ unsigned long long s_cls[NB_COUNT], s_anz[NB_COUNT], s_prod[NB_COUNT];
-  if (threadIdx.x < NB_COUNT) {
-    s_cls[threadIdx.x] = 0ull;
-    s_anz[threadIdx.x] = 0ull;
-    s_prod[threadIdx.x] = 0ull;
-  }
+  __shared__ unsigned long long s_cls[3][NB_COUNT];
+  if (threadIdx.x < 3 * NB_COUNT) (&s_cls[0][0])[threadIdx.x] = 0ull;
   const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * 4;
   uint32_t v[4];
   unsigned long long s = 0;
@@ -927,6 +1024,8 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
   }
   unsigned long long total;
   unsigned long long run = block_excl_scan<1024, unsigned long long>(s, scr, &total) + tile_offs[blockIdx.x];
+  // per-class sums of this thread's rows (nnz, A entries, products)
+  unsigned long long my_nnz[NB_COUNT] = {0}, my_anz[NB_COUNT] = {0}, my_prod[NB_COUNT] = {0};
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const uint64_t i = base + q;
@@ -938,19 +1037,35 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
       const uint32_t p = prod[i];
       b = num_bin_for(v[q], p, (uint64_t)hi[i] - lo[i] + 1, pol);
       if (b >= 0 && pol.force_bin < 0 && bm_off[i] != ~0ull) b = NB_BITMAP;  // reuse the saved bitmap
-      if (b >= 0) {
-        atomicAdd(&s_cls[b], (unsigned long long)v[q]);
-        atomicAdd(&s_anz[b], (unsigned long long)anz[i]);
-        atomicAdd(&s_prod[b], (unsigned long long)p);
+#pragma unroll
+      for (int c = 0; c < NB_COUNT; ++c) {
+        if (b == c) {
+          my_nnz[c] += v[q];
+          my_anz[c] += anz[i];
+          my_prod[c] += p;
+        }
       }
     }
     bin_append(b, (uint32_t)i, ctr->num_count, num_bins, n);
   }
+  // warp sums first, then one shared atomic per warp and class
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 0; c < NB_COUNT; ++c) {
+    const unsigned long long a = warp_sum_u64(my_nnz[c]);
+    const unsigned long long b2 = warp_sum_u64(my_anz[c]);
+    const unsigned long long d = warp_sum_u64(my_prod[c]);
+    if (lane == 0 && a) {
+      atomicAdd(&s_cls[0][c], a);
+      atomicAdd(&s_cls[1][c], b2);
+      atomicAdd(&s_cls[2][c], d);
+    }
+  }
   __syncthreads();
-  if (threadIdx.x < NB_COUNT && s_cls[threadIdx.x]) {
-    atomicAdd(&ctr->num_nnz[threadIdx.x], s_cls[threadIdx.x]);
-    atomicAdd(&ctr->num_anz[threadIdx.x], s_anz[threadIdx.x]);
-    atomicAdd(&ctr->num_prod[threadIdx.x], s_prod[threadIdx.x]);
+  if (threadIdx.x < NB_COUNT && s_cls[0][threadIdx.x]) {
+    atomicAdd(&ctr->num_nnz[threadIdx.x], s_cls[0][threadIdx.x]);
+    atomicAdd(&ctr->num_anz[threadIdx.x], s_cls[1][threadIdx.x]);
+    atomicAdd(&ctr->num_prod[threadIdx.x], s_cls[2][threadIdx.x]);
   }
 }
 
@@ -989,8 +1104,9 @@ constexpr size_t num_hash_smem() { return sizeof(NumHashSmem<NT, LOG2T>); }
 template <int NT, int LOG2T>
 constexpr size_t sym_hash_smem() { return sizeof(SymHashSmem<NT, LOG2T>); }
 
-int g_occ[16];  // resident blocks per SM of each persistent kernel (same order as kinds)
-enum Kind { K_SYM_ESC, K_SYM_S, K_SYM_M, K_SYM_L, K_SYM_BM, K_NUM_ESC, K_NUM_S, K_NUM_M, K_NUM_L, K_NUM_BM };
+int g_occ[24];  // resident blocks per SM of each persistent kernel (same order as kinds)
+enum Kind { K_SYM_ESC1, K_SYM_ESC2, K_SYM_ESC4, K_SYM_S, K_SYM_M, K_SYM_L, K_SYM_BM,
+            K_NUM_ESC1, K_NUM_ESC2, K_NUM_ESC4, K_NUM_S, K_NUM_M, K_NUM_L, K_NUM_BM };
 
 template <typename F>
 int occ_of(F f, int threads, size_t smem) {
@@ -1020,12 +1136,16 @@ void set_attrs() {
 void configure_kernel_attributes() {
   set_attrs<uint32_t>();
   set_attrs<uint64_t>();
-  g_occ[K_SYM_ESC] = occ_of(k_sym_esc<uint32_t>, 256, 0);
+  g_occ[K_SYM_ESC1] = occ_of(k_sym_esc<uint32_t, 1>, 256, 0);
+  g_occ[K_SYM_ESC2] = occ_of(k_sym_esc<uint32_t, 2>, 256, 0);
+  g_occ[K_SYM_ESC4] = occ_of(k_sym_esc<uint32_t, 4>, 256, 0);
   g_occ[K_SYM_S] = occ_of(k_sym_hash<uint32_t, 128, 11>, 128, sym_hash_smem<128, 11>());
   g_occ[K_SYM_M] = occ_of(k_sym_hash<uint32_t, 256, 13>, 256, sym_hash_smem<256, 13>());
   g_occ[K_SYM_L] = occ_of(k_sym_hash<uint32_t, 512, 15>, 512, sym_hash_smem<512, 15>());
   g_occ[K_SYM_BM] = occ_of(k_sym_bitmap<uint32_t>, kBitmapThreads, kSymBitmapSmem);
-  g_occ[K_NUM_ESC] = occ_of(k_num_esc<uint32_t>, 256, 0);
+  g_occ[K_NUM_ESC1] = occ_of(k_num_esc<uint32_t, 1>, 256, 0);
+  g_occ[K_NUM_ESC2] = occ_of(k_num_esc<uint32_t, 2>, 256, 0);
+  g_occ[K_NUM_ESC4] = occ_of(k_num_esc<uint32_t, 4>, 256, 0);
   g_occ[K_NUM_S] = occ_of(k_num_hash<uint32_t, 128, 10>, 128, num_hash_smem<128, 10>());
   g_occ[K_NUM_M] = occ_of(k_num_hash<uint32_t, 256, 12>, 256, num_hash_smem<256, 12>());
   g_occ[K_NUM_L] = occ_of(k_num_hash<uint32_t, 512, 13>, 512, num_hash_smem<512, 13>());
@@ -1033,9 +1153,9 @@ void configure_kernel_attributes() {
 }
 
 template <typename RP>
-void launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
-                     cudaStream_t s) {
-  if (A.rows == 0) return;
+int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
+                    cudaStream_t s) {
+  if (A.rows == 0) return 0;
   const double avg = (double)A.nnz / (double)A.rows;
   if (avg >= 12.0) {
     const uint64_t threads = A.rows * 32;
@@ -1046,64 +1166,109 @@ void launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const
     k_analysis<RP, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
         A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
   }
+  return 1;
+}
+
+// Grid of a persistent class kernel: resident blocks on all SMs, capped by
+// the class's work items (rows, or warps of rows for warp kernels).
+inline unsigned class_grid(int num_sms, int occ, const unsigned* counts, int cls, unsigned rows_per_block) {
+  const unsigned full = (unsigned)(num_sms * occ);
+  if (!counts) return full;
+  const unsigned need = (counts[cls] + rows_per_block - 1) / rows_per_block;
+  return need < full ? need : full;
 }
 
 template <typename RP>
-void launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms, cudaStream_t s,
-                     cudaEvent_t* ev) {
-  if (A.rows == 0) return;
+int launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms, cudaStream_t s,
+                    cudaEvent_t* ev, const unsigned* counts) {
+  if (A.rows == 0) return 0;
+  int launched = 0;
   auto mark = [&](int i) {
     if (ev) cudaEventRecord(ev[i], s);
   };
-  mark(0);
-  k_sym_esc<RP><<<num_sms * g_occ[K_SYM_ESC], 256, 0, s>>>(A, B, w.sym_bins, w.ctr, w.row_nnz);
-  mark(1);
-  k_sym_hash<RP, 128, 11><<<num_sms * g_occ[K_SYM_S], 128, sym_hash_smem<128, 11>(), s>>>(
-      A, B, w.sym_bins, w.ctr, SB_HASH_S, w.prod, w.row_nnz);
-  mark(2);
-  k_sym_hash<RP, 256, 13><<<num_sms * g_occ[K_SYM_M], 256, sym_hash_smem<256, 13>(), s>>>(
-      A, B, w.sym_bins, w.ctr, SB_HASH_M, w.prod, w.row_nnz);
-  mark(3);
-  k_sym_hash<RP, 512, 15><<<num_sms * g_occ[K_SYM_L], 512, sym_hash_smem<512, 15>(), s>>>(
-      A, B, w.sym_bins, w.ctr, SB_HASH_L, w.prod, w.row_nnz);
-  mark(4);
-  k_sym_bitmap<RP><<<num_sms * g_occ[K_SYM_BM], kBitmapThreads, kSymBitmapSmem, s>>>(
-      A, B, w.sym_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz, w.bm_off, w.bm_cache, w.bm_cache_words);
-  mark(5);
+  auto grid = [&](int kind, int cls, unsigned per_block) {
+    return class_grid(num_sms, g_occ[kind], counts, cls, per_block);
+  };
+  unsigned gsz;
+  mark(SB_ESC1);
+  if ((gsz = grid(K_SYM_ESC1, SB_ESC1, 8)) && ++launched)
+    k_sym_esc<RP, 1><<<gsz, 256, 0, s>>>(A, B, w.sym_bins, w.ctr, SB_ESC1, w.row_nnz);
+  mark(SB_ESC2);
+  if ((gsz = grid(K_SYM_ESC2, SB_ESC2, 8)) && ++launched)
+    k_sym_esc<RP, 2><<<gsz, 256, 0, s>>>(A, B, w.sym_bins, w.ctr, SB_ESC2, w.row_nnz);
+  mark(SB_ESC4);
+  if ((gsz = grid(K_SYM_ESC4, SB_ESC4, 8)) && ++launched)
+    k_sym_esc<RP, 4><<<gsz, 256, 0, s>>>(A, B, w.sym_bins, w.ctr, SB_ESC4, w.row_nnz);
+  mark(SB_HASH_S);
+  if ((gsz = grid(K_SYM_S, SB_HASH_S, 1)) && ++launched)
+    k_sym_hash<RP, 128, 11><<<gsz, 128, sym_hash_smem<128, 11>(), s>>>(A, B, w.sym_bins, w.ctr, SB_HASH_S, w.prod,
+                                                                       w.row_nnz);
+  mark(SB_HASH_M);
+  if ((gsz = grid(K_SYM_M, SB_HASH_M, 1)) && ++launched)
+    k_sym_hash<RP, 256, 13><<<gsz, 256, sym_hash_smem<256, 13>(), s>>>(A, B, w.sym_bins, w.ctr, SB_HASH_M, w.prod,
+                                                                       w.row_nnz);
+  mark(SB_HASH_L);
+  if ((gsz = grid(K_SYM_L, SB_HASH_L, 1)) && ++launched)
+    k_sym_hash<RP, 512, 15><<<gsz, 512, sym_hash_smem<512, 15>(), s>>>(A, B, w.sym_bins, w.ctr, SB_HASH_L, w.prod,
+                                                                       w.row_nnz);
+  mark(SB_BITMAP);
+  if ((gsz = grid(K_SYM_BM, SB_BITMAP, 1)) && ++launched)
+    k_sym_bitmap<RP><<<gsz, kBitmapThreads, kSymBitmapSmem, s>>>(A, B, w.sym_bins, w.ctr, w.prod, w.lo, w.hi,
+                                                                 w.row_nnz, w.bm_off, w.bm_cache, w.bm_cache_words);
+  mark(SB_COUNT);
+  return launched;
 }
 
-void launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s) {
+int launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s) {
   const uint64_t nt = scan_tiles(w.rows);
-  if (w.rows == 0) return;
+  if (w.rows == 0) return 0;
   k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums);
   k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, w.ctr, w.rowptr64, w.rowptr32, w.rows);
   k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums, w.rowptr64, w.rowptr32,
                                              w.prod, w.lo, w.hi, w.anz, w.bm_off, w.num_bins, w.ctr, pol);
+  return 3;
 }
 
 template <typename RP>
-void launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_t* c_col, double* c_val,
-                    int num_sms, cudaStream_t s, cudaEvent_t* ev) {
-  if (A.rows == 0) return;
+int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_t* c_col, double* c_val,
+                   int num_sms, cudaStream_t s, cudaEvent_t* ev, const unsigned* counts) {
+  if (A.rows == 0) return 0;
+  int launched = 0;
   auto mark = [&](int i) {
     if (ev) cudaEventRecord(ev[i], s);
   };
-  mark(0);
-  k_num_esc<RP><<<num_sms * g_occ[K_NUM_ESC], 256, 0, s>>>(A, B, w.num_bins, w.ctr, w.row_nnz,
-                                                            w.rowptr64, c_col, c_val);
-  mark(1);
-  k_num_hash<RP, 128, 10><<<num_sms * g_occ[K_NUM_S], 128, num_hash_smem<128, 10>(), s>>>(
-      A, B, w.num_bins, w.ctr, NB_HASH_S, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
-  mark(2);
-  k_num_hash<RP, 256, 12><<<num_sms * g_occ[K_NUM_M], 256, num_hash_smem<256, 12>(), s>>>(
-      A, B, w.num_bins, w.ctr, NB_HASH_M, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
-  mark(3);
-  k_num_hash<RP, 512, 13><<<num_sms * g_occ[K_NUM_L], 512, num_hash_smem<512, 13>(), s>>>(
-      A, B, w.num_bins, w.ctr, NB_HASH_L, w.prod, w.row_nnz, w.rowptr64, c_col, c_val);
-  mark(4);
-  k_num_bitmap<RP><<<num_sms * g_occ[K_NUM_BM], kBitmapThreads, kNumBitmapSmem, s>>>(
-      A, B, w.num_bins, w.ctr, w.prod, w.lo, w.hi, w.row_nnz, w.rowptr64, w.bm_off, w.bm_cache, c_col, c_val);
-  mark(5);
+  auto grid = [&](int kind, int cls, unsigned per_block) {
+    return class_grid(num_sms, g_occ[kind], counts, cls, per_block);
+  };
+  unsigned gsz;
+  mark(NB_ESC1);
+  if ((gsz = grid(K_NUM_ESC1, NB_ESC1, 8)) && ++launched)
+    k_num_esc<RP, 1><<<gsz, 256, 0, s>>>(A, B, w.num_bins, w.ctr, NB_ESC1, w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(NB_ESC2);
+  if ((gsz = grid(K_NUM_ESC2, NB_ESC2, 8)) && ++launched)
+    k_num_esc<RP, 2><<<gsz, 256, 0, s>>>(A, B, w.num_bins, w.ctr, NB_ESC2, w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(NB_ESC4);
+  if ((gsz = grid(K_NUM_ESC4, NB_ESC4, 8)) && ++launched)
+    k_num_esc<RP, 4><<<gsz, 256, 0, s>>>(A, B, w.num_bins, w.ctr, NB_ESC4, w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(NB_HASH_S);
+  if ((gsz = grid(K_NUM_S, NB_HASH_S, 1)) && ++launched)
+    k_num_hash<RP, 128, 10><<<gsz, 128, num_hash_smem<128, 10>(), s>>>(A, B, w.num_bins, w.ctr, NB_HASH_S, w.prod,
+                                                                       w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(NB_HASH_M);
+  if ((gsz = grid(K_NUM_M, NB_HASH_M, 1)) && ++launched)
+    k_num_hash<RP, 256, 12><<<gsz, 256, num_hash_smem<256, 12>(), s>>>(A, B, w.num_bins, w.ctr, NB_HASH_M, w.prod,
+                                                                       w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(NB_HASH_L);
+  if ((gsz = grid(K_NUM_L, NB_HASH_L, 1)) && ++launched)
+    k_num_hash<RP, 512, 13><<<gsz, 512, num_hash_smem<512, 13>(), s>>>(A, B, w.num_bins, w.ctr, NB_HASH_L, w.prod,
+                                                                       w.row_nnz, w.rowptr64, c_col, c_val);
+  mark(NB_BITMAP);
+  if ((gsz = grid(K_NUM_BM, NB_BITMAP, 1)) && ++launched)
+    k_num_bitmap<RP><<<gsz, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, w.num_bins, w.ctr, w.prod, w.lo, w.hi,
+                                                                 w.row_nnz, w.rowptr64, w.bm_off, w.bm_cache, c_col,
+                                                                 c_val);
+  mark(NB_COUNT);
+  return launched;
 }
 
 void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, cudaStream_t s) {
@@ -1112,17 +1277,17 @@ void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t se
   k_murmur3<<<(unsigned)(blocks > 4096 ? 4096 : blocks), 256, 0, s>>>(keys, out, n, seed);
 }
 
-template void launch_analysis<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
+template int launch_analysis<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
                                         const SymPolicy&, cudaStream_t);
-template void launch_analysis<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
+template int launch_analysis<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
                                         const SymPolicy&, cudaStream_t);
-template void launch_symbolic<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, int,
-                                        cudaStream_t, cudaEvent_t*);
-template void launch_symbolic<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, int,
-                                        cudaStream_t, cudaEvent_t*);
-template void launch_numeric<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
-                                       uint32_t*, double*, int, cudaStream_t, cudaEvent_t*);
-template void launch_numeric<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
-                                       uint32_t*, double*, int, cudaStream_t, cudaEvent_t*);
+template int launch_symbolic<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, int,
+                                        cudaStream_t, cudaEvent_t*, const unsigned*);
+template int launch_symbolic<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, int,
+                                        cudaStream_t, cudaEvent_t*, const unsigned*);
+template int launch_numeric<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
+                                       uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*);
+template int launch_numeric<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
+                                       uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*);
 
 }  // namespace ocean

@@ -65,8 +65,8 @@ enum Ev {
   EV_COUNT
 };
 
-const char* const kSymNames[SB_COUNT] = {"esc", "hash_s", "hash_m", "hash_l", "bitmap"};
-const char* const kNumNames[NB_COUNT] = {"esc", "hash_s", "hash_m", "hash_l", "bitmap"};
+const char* const kSymNames[SB_COUNT] = {"esc1", "esc2", "esc4", "hash_s", "hash_m", "hash_l", "bitmap"};
+const char* const kNumNames[NB_COUNT] = {"esc1", "esc2", "esc4", "hash_s", "hash_m", "hash_l", "bitmap"};
 
 struct Stats {
   uint64_t a_rows = 0, a_cols = 0, a_nnz = 0, b_rows = 0, b_cols = 0, b_nnz = 0;
@@ -82,6 +82,7 @@ struct Stats {
   uint64_t sym_prod[SB_COUNT] = {0};
   uint64_t cache_words = 0, cache_used = 0;
   bool cache_dropped = false;
+  int launches = 0;  // kernels launched by the last call
   int workflow = 0;  // 0 = precise (symbolic + numeric)
   int rowptr_bits = 32;
   bool valid = false;
@@ -296,12 +297,15 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   h->w.bm_cache = nullptr;
   h->w.bm_cache_words = 0;
   record(h, EV_START, s);
-  launch_analysis(A, B, h->w, sp, s);
+  h->st.launches = launch_analysis(A, B, h->w, sp, s);
   OCEAN_CUDA(cudaGetLastError());
   record(h, EV_ANALYSIS, s);
+  // the class sizes decide which class kernels run and how big the bitmap cache is
+  OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+  OCEAN_CUDA(cudaStreamSynchronize(s));
+  unsigned sym_counts[SB_COUNT];
+  for (int i = 0; i < SB_COUNT; ++i) sym_counts[i] = h->h_ctr->sym_count[i];
   if (allow_cache && h->cfg.bitmap_cache_fraction > 0.0) {
-    OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
-    OCEAN_CUDA(cudaStreamSynchronize(s));
     const uint64_t want = h->h_ctr->sym_words;
     const uint64_t budget = (uint64_t)(h->cfg.bitmap_cache_fraction * (double)available_device_bytes(h->device)) / 8;
     const uint64_t words = std::min(want, budget);
@@ -323,10 +327,10 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
       }
     }
   }
-  launch_symbolic(A, B, h->w, h->num_sms, s, h->ev + EV_SYM0);
+  h->st.launches += launch_symbolic(A, B, h->w, h->num_sms, s, h->ev + EV_SYM0, sym_counts);
   OCEAN_CUDA(cudaGetLastError());
   if (with_scan) {
-    launch_scan(h->w, np, s);
+    h->st.launches += launch_scan(h->w, np, s);
     OCEAN_CUDA(cudaGetLastError());
   }
   record(h, EV_SCAN, s);
@@ -404,7 +408,9 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     }
     OCEAN_CUDA(e);
     if (A.rows > 0) {
-      launch_numeric(A, B, h->w, owner->col, owner->val, h->num_sms, s, h->ev + EV_NUM0);
+      unsigned num_counts[NB_COUNT];
+      for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
+      st.launches += launch_numeric(A, B, h->w, owner->col, owner->val, h->num_sms, s, h->ev + EV_NUM0, num_counts);
       OCEAN_CUDA(cudaGetLastError());
       OCEAN_CUDA(cudaMemcpyAsync(owner->rowptr, bits == 64 ? (void*)h->w.rowptr64 : (void*)h->w.rowptr32,
                                  (A.rows + 1) * (bits / 8), cudaMemcpyDeviceToDevice, s));
@@ -517,7 +523,8 @@ std::string stats_json(ocean_handle* h) {
     << ", \"max_a_row_nnz\": " << st.max_a_nnz << "}, ";
   o << "\"decision\": {\"workflow\": " << st.workflow << ", \"rowptr_bits\": " << st.rowptr_bits
     << ", \"bitmap_cache_bytes\": " << 8 * st.cache_words << ", \"bitmap_cache_used_bytes\": " << 8 * st.cache_used
-    << ", \"bitmap_cache_dropped\": " << (st.cache_dropped ? "true" : "false") << "}, ";
+    << ", \"bitmap_cache_dropped\": " << (st.cache_dropped ? "true" : "false")
+    << ", \"kernel_launches\": " << st.launches << "}, ";
   o << "\"binning_1\": [";
   for (int i = 0; i < SB_COUNT; ++i) o << (i ? ", " : "") << st.sym_bins[i];
   o << "], \"binning_2\": [";

@@ -21,20 +21,24 @@ constexpr int kSupers = kBitmapWords / kSuperWords;     // 16
 // Row classes ("bins"). Symbolic classes are chosen from the product count and
 // the column span, numeric classes from the exact output count.
 enum SymBin : int {
-  SB_ESC = 0,      // <= 32 products: one warp, match-any distinct count
-  SB_HASH_S = 1,   // hash set, 128 threads, 2048 slots
-  SB_HASH_M = 2,   // hash set, 256 threads, 8192 slots
-  SB_HASH_L = 3,   // hash set, 512 threads, 32768 slots
-  SB_BITMAP = 4,   // bitmap over the column span, 1024 threads
-  SB_COUNT = 5
+  SB_ESC1 = 0,     // <= 32 products: one warp, 1 product per lane, register sort + distinct count
+  SB_ESC2 = 1,     // <= 64 products: one warp, 2 per lane
+  SB_ESC4 = 2,     // <= 128 products: one warp, 4 per lane
+  SB_HASH_S = 3,   // hash set, 128 threads, 2048 slots
+  SB_HASH_M = 4,   // hash set, 256 threads, 8192 slots
+  SB_HASH_L = 5,   // hash set, 512 threads, 32768 slots
+  SB_BITMAP = 6,   // bitmap over the column span, 1024 threads
+  SB_COUNT = 7
 };
 enum NumBin : int {
-  NB_ESC = 0,      // <= 32 products: one warp, register sort + segmented sum
-  NB_HASH_S = 1,   // hash accumulate + sort, 128 threads, 1024 slots (<= 512 out)
-  NB_HASH_M = 2,   // 256 threads, 4096 slots (<= 2048 out)
-  NB_HASH_L = 3,   // 512 threads, 8192 slots (<= 4096 out)
-  NB_BITMAP = 4,   // bitmap-rank accumulator, any size
-  NB_COUNT = 5
+  NB_ESC1 = 0,     // <= 32 products: one warp, register sort + segmented sum
+  NB_ESC2 = 1,     // <= 64 products
+  NB_ESC4 = 2,     // <= 128 products
+  NB_HASH_S = 3,   // hash accumulate + sort, 128 threads, 1024 slots (<= 512 out)
+  NB_HASH_M = 4,   // 256 threads, 4096 slots (<= 2048 out)
+  NB_HASH_L = 5,   // 512 threads, 8192 slots (<= 4096 out)
+  NB_BITMAP = 6,   // bitmap-rank accumulator, any size
+  NB_COUNT = 7
 };
 
 // Device-side counters of one multiply (zeroed at the start of each call).

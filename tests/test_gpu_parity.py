@@ -11,8 +11,8 @@ from research_b200.ocean import DeviceCSR, HostCSR, OceanError, SpGEMM
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
-SYM_BINS = {"esc": 0, "hash_s": 1, "hash_m": 2, "hash_l": 3, "bitmap": 4}
-NUM_BINS = {"esc": 0, "hash_s": 1, "hash_m": 2, "hash_l": 3, "bitmap": 4}
+SYM_BINS = {"esc1": 0, "esc2": 1, "esc4": 2, "hash_s": 3, "hash_m": 4, "hash_l": 5, "bitmap": 6}
+NUM_BINS = {"esc1": 0, "esc2": 1, "esc4": 2, "hash_s": 3, "hash_m": 4, "hash_l": 5, "bitmap": 6}
 
 
 def multiply_device(A, B, config=None):
@@ -56,16 +56,16 @@ def test_laplacian_256_full():
     assert st["C"]["nnz"] == 846852 and st["stats"]["intermediate_product"] == 1629192
 
 
-@pytest.mark.parametrize("sym", ["hash_s", "hash_m", "hash_l", "bitmap"])
-@pytest.mark.parametrize("num", ["hash_s", "hash_m", "hash_l", "bitmap"])
-def test_forced_classes_rmat(sym, num):
+@pytest.mark.parametrize("sym", ["esc4", "hash_s", "hash_m", "hash_l", "bitmap"])
+@pytest.mark.parametrize("num", ["esc4", "hash_s", "hash_m", "hash_l", "bitmap"])
+def test_forced_classes_uniform(sym, num):
     A = M.uniform_random(6000, 10, seed=11)
     # keep every row within the forced classes' capacities
     prod, _, _ = O.row_stats(A, A)
     cnt = O.symbolic(A, A)
-    caps_sym = {"hash_s": 1024, "hash_m": 4096, "hash_l": 16384, "bitmap": 1 << 40}
-    caps_num = {"hash_s": 512, "hash_m": 2048, "hash_l": 4096, "bitmap": 1 << 40}
-    if prod.max() > caps_sym[sym] or cnt.max() > caps_num[num]:
+    caps_sym = {"esc4": 128, "hash_s": 1024, "hash_m": 4096, "hash_l": 16384, "bitmap": 1 << 40}
+    caps_num = {"esc4": 128, "hash_s": 512, "hash_m": 2048, "hash_l": 4096, "bitmap": 1 << 40}
+    if prod.max() > caps_sym[sym] or cnt.max() > caps_num[num] or (num == "esc4" and prod.max() > 128):
         pytest.skip("matrix exceeds the forced class capacity")
     C, _ = multiply_device(A, A, {"force_sym_bin": SYM_BINS[sym], "force_num_bin": NUM_BINS[num]})
     check(A, A, C)
@@ -112,9 +112,9 @@ def test_wide_span_multi_window():
     A = M.from_coo(200, rows, np.repeat(np.arange(200), 24), rng.integers(0, rows, 200 * 24),
                    rng.uniform(-1, 1, 200 * 24))
     for num in ("bitmap", None):
-        cfg = {"force_sym_bin": 4} if num else {}
+        cfg = {"force_sym_bin": SYM_BINS["bitmap"]} if num else {}
         if num:
-            cfg["force_num_bin"] = 4
+            cfg["force_num_bin"] = NUM_BINS["bitmap"]
         C, _ = multiply_device(A, B, cfg)
         check(A, B, C)
 
@@ -128,7 +128,7 @@ def test_hub_rows_large_products():
     A = M.from_coo(300, n, r, rng.integers(0, n, r.size), rng.uniform(-1, 1, r.size))
     C, st = multiply_device(A, B)
     check(A, B, C)
-    assert st["binning_2"][4] >= 4
+    assert st["binning_2"][NUM_BINS["bitmap"]] >= 4
 
 
 def test_rowptr_64_and_mixed_inputs():
@@ -177,7 +177,7 @@ def test_errors_are_status_codes():
     # a row forced into a class too small for it is reported, not mis-written
     R = M.block_diagonal(4096, 1024, 64, seed=2)
     with pytest.raises(OceanError) as e:
-        multiply_device(R, R, {"force_num_bin": 1})
+        multiply_device(R, R, {"force_num_bin": NUM_BINS["hash_s"]})
     assert e.value.code in (2, 6)
 
 
@@ -225,3 +225,36 @@ def test_bitmap_cache_on_and_off(frac):
     check(A, A, C)
     used = st["decision"]["bitmap_cache_used_bytes"]
     assert (used > 0) == (frac > 0)
+
+
+@pytest.mark.parametrize("k", [1, 2, 4])
+def test_esc_classes_with_repeated_columns(k):
+    # rows whose products repeat the same column many times, across register
+    # rows of the warp sort (runs longer than 32), and cancelling sums
+    rng = np.random.default_rng(40 + k)
+    n = 64
+    cap = 32 * k
+    B = M.from_coo(n, 50, np.repeat(np.arange(n), 3), rng.integers(0, 6, 3 * n), rng.uniform(-1, 1, 3 * n))
+    nb = np.diff(B.rowptr.astype(np.int64))
+    rows, cols = [], []
+    for i in range(300):
+        budget = int(rng.integers(1, cap + 1))
+        picked, tot = [], 0
+        for j in rng.permutation(n):
+            if tot + nb[j] > budget:
+                continue
+            picked.append(j)
+            tot += nb[j]
+        rows += [i] * len(picked)
+        cols += picked
+    A = M.from_coo(300, n, rows, cols, rng.uniform(-1, 1, len(rows)))
+    cls = {1: "esc1", 2: "esc2", 4: "esc4"}[k]
+    C, st = multiply_device(A, B, {"force_sym_bin": SYM_BINS[cls], "force_num_bin": NUM_BINS[cls]})
+    check(A, B, C)
+
+
+def test_esc_overflow_is_reported():
+    A = M.block_diagonal(2048, 256, 32, seed=5)  # 1024 products per row
+    with pytest.raises(OceanError) as e:
+        multiply_device(A, A, {"force_sym_bin": SYM_BINS["esc4"]})
+    assert e.value.code in (2, 6)
