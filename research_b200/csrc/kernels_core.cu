@@ -161,10 +161,25 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     } else {
       const uint64_t span = (uint64_t)mx - mn + 1;
       b = sym_bin_for(p, span, pol);
-      atomicAdd(&s_anz[b], (unsigned long long)(a1 - a0));
-      atomicAdd(&s_prod[b], p);
-      if (b == SB_BITMAP && span <= kBitmapBits) atomicAdd(&s_words, (unsigned long long)((span + 63) >> 6));
     }
+  }
+  {
+    // per-class sums: warp reductions first, one shared atomic per warp and class
+    const unsigned long long my_anz = (b >= 0) ? (unsigned long long)(a1 - a0) : 0ull;
+    const unsigned long long my_p = (b >= 0) ? p : 0ull;
+    const uint64_t span = (uint64_t)mx - mn + 1;
+    const unsigned long long my_w = (b == SB_BITMAP && span <= kBitmapBits) ? ((span + 63) >> 6) : 0ull;
+#pragma unroll
+    for (int c = 0; c < SB_COUNT; ++c) {
+      const unsigned long long sa = warp_sum_u64(b == c ? my_anz : 0ull);
+      const unsigned long long sp = warp_sum_u64(b == c ? my_p : 0ull);
+      if (lane == 0 && sp) {
+        atomicAdd(&s_anz[c], sa);
+        atomicAdd(&s_prod[c], sp);
+      }
+    }
+    const unsigned long long sw = warp_sum_u64(my_w);
+    if (lane == 0 && sw) atomicAdd(&s_words, sw);
   }
   bin_append(b, (uint32_t)row, ctr->sym_count, sym_bins, A.rows);
   // totals for stats and the workflow decision

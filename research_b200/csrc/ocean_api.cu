@@ -299,7 +299,7 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   record(h, EV_START, s);
   h->st.launches = launch_analysis(A, B, h->w, sp, s);
   OCEAN_CUDA(cudaGetLastError());
-  record(h, EV_ANALYSIS, s);
+  if (h->cfg.track_stage_times) record(h, EV_ANALYSIS, s);
   // the class sizes decide which class kernels run and how big the bitmap cache is
   OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
   OCEAN_CUDA(cudaStreamSynchronize(s));
@@ -327,13 +327,15 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
       }
     }
   }
-  h->st.launches += launch_symbolic(A, B, h->w, h->num_sms, s, h->ev + EV_SYM0, sym_counts);
+  // per-class boundary events only when stage timing is asked for (each record costs device time)
+  const bool track = h->cfg.track_stage_times;
+  h->st.launches += launch_symbolic(A, B, h->w, h->num_sms, s, track ? h->ev + EV_SYM0 : nullptr, sym_counts);
   OCEAN_CUDA(cudaGetLastError());
   if (with_scan) {
     h->st.launches += launch_scan(h->w, np, s);
     OCEAN_CUDA(cudaGetLastError());
   }
-  record(h, EV_SCAN, s);
+  if (h->cfg.track_stage_times) record(h, EV_SCAN, s);
   OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
   OCEAN_CUDA(cudaStreamSynchronize(s));
   check_device_status(h);
@@ -410,7 +412,8 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     if (A.rows > 0) {
       unsigned num_counts[NB_COUNT];
       for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
-      st.launches += launch_numeric(A, B, h->w, owner->col, owner->val, h->num_sms, s, h->ev + EV_NUM0, num_counts);
+      st.launches += launch_numeric(A, B, h->w, owner->col, owner->val, h->num_sms, s,
+                                    h->cfg.track_stage_times ? h->ev + EV_NUM0 : nullptr, num_counts);
       OCEAN_CUDA(cudaGetLastError());
       OCEAN_CUDA(cudaMemcpyAsync(owner->rowptr, bits == 64 ? (void*)h->w.rowptr64 : (void*)h->w.rowptr32,
                                  (A.rows + 1) * (bits / 8), cudaMemcpyDeviceToDevice, s));
