@@ -107,6 +107,21 @@ int ocean_csr_download_rows(const ocean_csr* C, uint64_t r0, uint64_t r1, uint64
 int ocean_symbolic(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B,
                    uint32_t* row_nnz, void* stream);
 
+/* ocean_symbolic without any allocation by the library, for callers that
+ * cannot let a library allocate device memory (an application-owned arena or
+ * caching allocator holds the device memory; or a service forbids cudaMalloc in
+ * steady state because it can synchronize the device). No handle: the scratch
+ * of the analysis and symbolic kernels is one fixed device array inside the
+ * library (about 6.8 MB, held by every GPU that loads the library until exit),
+ * so A may have at most 131072 rows (larger A: OCEAN_ERR_INVALID). A and B need
+ * the same row-pointer width; row_nnz[A.rows] is the caller's device array. The
+ * first call on a device resolves the array's address and must come before any
+ * stream capture. Calls share the array: calls that overlap on the GPU race and
+ * must be ordered by the caller. Waits for the result before returning.
+ * No counterpart in the reference (which allocates on every run). */
+int ocean_symbolic_noalloc(const ocean_csr_view* A, const ocean_csr_view* B, uint32_t* row_nnz,
+                           void* stream);
+
 /* Stats of the last multiply as JSON text, with the reference's keys
  * (kernels/SpGEMM.cuh:1788-1890: "A","B","C","stats","decision","timing",
  * "total_time","gflops", ...). If cap is too small, *needed gets the size. */

@@ -61,4 +61,7 @@ void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t se
 // Per-kernel dynamic shared memory opt-in; call once per device.
 void configure_kernel_attributes();
 
+// Stores the calling thread's error message returned by ocean_last_error().
+void set_last_error(const char* msg);
+
 }  // namespace ocean

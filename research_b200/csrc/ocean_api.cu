@@ -580,6 +580,10 @@ int guarded(F&& f) {
 
 }  // namespace
 
+namespace ocean {
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+}  // namespace ocean
+
 extern "C" {
 
 int ocean_create(ocean_handle** out, const char* json_config) {
