@@ -187,6 +187,8 @@ struct Config {
   int force_num_bin = -1;         // testing: put every non-empty row in one numeric class
   bool sync_on_return = true;     // check device status before returning
   double bitmap_cache_fraction = 0.25;  // share of free device memory the saved row bitmaps may use
+  int small_problem_nnz = 1 << 20;      // A with at most this many entries: no read-back after analysis
+  int spin_wait_us = 2000;              // poll the stream this long before a blocking synchronize
 
   static Config from_json_text(const std::string& text) {
     Config c;
@@ -248,6 +250,8 @@ struct Config {
     geti("force_num_bin", c.force_num_bin);
     getb("sync_on_return", c.sync_on_return);
     getd("bitmap_cache_fraction", c.bitmap_cache_fraction);
+    geti("small_problem_nnz", c.small_problem_nnz);
+    geti("spin_wait_us", c.spin_wait_us);
     if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
     if (c.bitmap_cache_fraction < 0.0 || c.bitmap_cache_fraction > 0.9)

@@ -232,6 +232,19 @@ void validate_view(const ocean_csr_view* m, const char* name) {
 
 void record(ocean_handle* h, int i, cudaStream_t s) { cudaEventRecord(h->ev[i], s); }
 
+// Waits for `s` by polling for a short, bounded time before falling back to a
+// blocking synchronize: the mid-call read-backs are tens of microseconds apart
+// on small problems, where a sleeping wait adds scheduler wake-up jitter.
+cudaError_t wait_stream(cudaStream_t s, int spin_us) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t e = cudaStreamQuery(s);
+    if (e != cudaErrorNotReady) return e;
+    if (std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() > spin_us)
+      return cudaStreamSynchronize(s);
+  }
+}
+
 const char* status_text(unsigned st) {
   if (st & DEV_TABLE_FULL) return "a shared-memory hash table ran full (probe limit reached)";
   if (st & DEV_BIN_OVERFLOW) return "a row exceeded the capacity of its accumulator class";
@@ -300,12 +313,17 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   h->st.launches = launch_analysis(A, B, h->w, sp, s);
   OCEAN_CUDA(cudaGetLastError());
   if (h->cfg.track_stage_times) record(h, EV_ANALYSIS, s);
-  // the class sizes decide which class kernels run and how big the bitmap cache is
-  OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
-  OCEAN_CUDA(cudaStreamSynchronize(s));
+  // The class sizes decide which class kernels run and how big the bitmap cache
+  // is. Small inputs skip this read-back: every class kernel is launched (empty
+  // ones exit at once) and no bitmaps are saved.
+  const bool readback = A.nnz > (uint64_t)h->cfg.small_problem_nnz;
   unsigned sym_counts[SB_COUNT];
-  for (int i = 0; i < SB_COUNT; ++i) sym_counts[i] = h->h_ctr->sym_count[i];
-  if (allow_cache && h->cfg.bitmap_cache_fraction > 0.0) {
+  if (readback) {
+    OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+    OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
+    for (int i = 0; i < SB_COUNT; ++i) sym_counts[i] = h->h_ctr->sym_count[i];
+  }
+  if (readback && allow_cache && h->cfg.bitmap_cache_fraction > 0.0) {
     const uint64_t want = h->h_ctr->sym_words;
     const uint64_t budget = (uint64_t)(h->cfg.bitmap_cache_fraction * (double)available_device_bytes(h->device)) / 8;
     const uint64_t words = std::min(want, budget);
@@ -329,7 +347,8 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   }
   // per-class boundary events only when stage timing is asked for (each record costs device time)
   const bool track = h->cfg.track_stage_times;
-  h->st.launches += launch_symbolic(A, B, h->w, h->num_sms, s, track ? h->ev + EV_SYM0 : nullptr, sym_counts);
+  h->st.launches += launch_symbolic(A, B, h->w, h->num_sms, s, track ? h->ev + EV_SYM0 : nullptr,
+                                    readback ? sym_counts : nullptr);
   OCEAN_CUDA(cudaGetLastError());
   if (with_scan) {
     h->st.launches += launch_scan(h->w, np, s);
@@ -337,7 +356,7 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   }
   if (h->cfg.track_stage_times) record(h, EV_SCAN, s);
   OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
-  OCEAN_CUDA(cudaStreamSynchronize(s));
+  OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
   check_device_status(h);
 }
 
@@ -427,7 +446,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     h->tracked = h->cfg.track_stage_times;
     if (h->cfg.sync_on_return && A.rows > 0) {
       OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
-      OCEAN_CUDA(cudaStreamSynchronize(s));
+      OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
       check_device_status(h);
     }
   } catch (...) {

@@ -71,8 +71,9 @@ def test_forced_classes_uniform(sym, num):
     check(A, A, C)
 
 
+@pytest.mark.parametrize("readback", [False, True])
 @pytest.mark.parametrize("gen", ["uniform", "banded", "block", "rmat14", "rect"])
-def test_families(gen):
+def test_families(gen, readback):
     if gen == "uniform":
         A = M.uniform_random(20000, 16, seed=1); B = A
     elif gen == "banded":
@@ -83,7 +84,9 @@ def test_families(gen):
         A = M.rmat(14, 16, seed=4); B = A
     else:
         A = M.rect_poisson(16384, 65536, 12.0, seed=5); B = M.transpose(A)
-    C, st = multiply_device(A, B)
+    # readback: class sizes read back after the analysis (selective launches, bitmap cache);
+    # otherwise the small-input mode that launches every class without a read-back
+    C, st = multiply_device(A, B, {"small_problem_nnz": 0 if readback else 1 << 30})
     check(A, B, C)
     assert sum(st["binning_2"]) == int(np.count_nonzero(np.diff(C.rowptr.astype(np.int64))))
 
@@ -221,7 +224,7 @@ def test_bitmap_cache_on_and_off(frac):
     # rows of the bitmap class either reload the bitmap saved by the symbolic
     # pass or mark their columns again; both must give the oracle's C
     A = M.rmat(15, 16, seed=3)
-    C, st = multiply_device(A, A, {"bitmap_cache_fraction": frac})
+    C, st = multiply_device(A, A, {"bitmap_cache_fraction": frac, "small_problem_nnz": 0})
     check(A, A, C)
     used = st["decision"]["bitmap_cache_used_bytes"]
     assert (used > 0) == (frac > 0)
