@@ -325,7 +325,8 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
   }
   if (readback && allow_cache && h->cfg.bitmap_cache_fraction > 0.0) {
     const uint64_t want = h->h_ctr->sym_words;
-    const uint64_t budget = (uint64_t)(h->cfg.bitmap_cache_fraction * (double)available_device_bytes(h->device)) / 8;
+    const uint64_t budget =
+        want >= 1024 ? (uint64_t)(h->cfg.bitmap_cache_fraction * (double)available_device_bytes(h->device)) / 8 : 0;
     const uint64_t words = std::min(want, budget);
     if (words >= 1024) {
       if (h->cache_cap_words < words) {
