@@ -107,6 +107,15 @@ int ocean_csr_download_rows(const ocean_csr* C, uint64_t r0, uint64_t r1, uint64
 int ocean_symbolic(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B,
                    uint32_t* row_nnz, void* stream);
 
+/* Raw HyperLogLog estimate of every row's output count into the device array
+ * est[A.rows]: register-wise maximum of the 2^log2p-register sketches
+ * (log2p 5 or 6, MurmurHash3 seed 1234) of the B rows each A row references,
+ * then the harmonic-mean estimate with small-range correction. Replaces
+ * hllConstruct + hllMerge (kernels/HLL.cuh:28-236) without the expansion and
+ * bin rounding. */
+int ocean_row_estimates(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, int log2p,
+                        uint32_t* est, void* stream);
+
 /* ocean_symbolic without any allocation by the library, for callers that
  * cannot let a library allocate device memory (an application-owned arena or
  * caching allocator holds the device memory; or a service forbids cudaMalloc in

@@ -246,9 +246,9 @@ void oracle_hll_sketch_rows(uint64_t rows, uint64_t nnz, const uint64_t* rp, con
 
 /* Raw HLL cardinality estimate of the union of the B-row sketches selected by
  * one A row (kernels/HLL.cuh:161-219): E = alpha*m^2 / sum 2^-M[i], replaced by
- * m*ln(m/V) when some registers are empty and E < 2.5m. The reference computes
- * the log with -use_fast_math on a float argument; this uses the libm log of
- * the same float, so results can differ by one. */
+ * m*ln(m/V) when some registers are empty and E < 2.5m. The reference takes
+ * that log of a float quotient with -use_fast_math, so its integer estimate can
+ * differ from this double-precision one by one; estimates only size buffers. */
 int64_t oracle_hll_estimate_union(const uint8_t* sketches, int log2p, const uint32_t* rows, uint64_t nrows) {
   static const double kAlpha[8] = {0.0, 0.0, 0.0, 0.0, 0.673, 0.697, 0.709, 0.715};
   const uint32_t m = 1u << log2p;
@@ -266,6 +266,6 @@ int64_t oracle_hll_estimate_union(const uint8_t* sketches, int log2p, const uint
     empty += reg[i] == 0;
   }
   int64_t result = (int64_t)(kAlpha[log2p] * m * m / z);
-  if (empty != 0 && result < 2.5 * m) result = (int64_t)(m * log((double)((float)m / (float)empty)));
+  if (empty != 0 && result < 2.5 * m) result = (int64_t)(m * log((double)m / (double)empty));
   return result;
 }

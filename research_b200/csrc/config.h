@@ -189,6 +189,8 @@ struct Config {
   double bitmap_cache_fraction = 0.25;  // share of free device memory the saved row bitmaps may use
   int small_problem_nnz = 1 << 20;      // A with at most this many entries: no read-back after analysis
   int spin_wait_us = 2000;              // poll the stream this long before a blocking synchronize
+  int force_workflow = -1;              // -1 auto; 0 precise, 1 estimation (HLL), 2 ultra-sparse
+  double estimate_scale = 1.0;          // multiplies the HLL expansion (testing: < 1 forces overflows)
 
   static Config from_json_text(const std::string& text) {
     Config c;
@@ -252,8 +254,13 @@ struct Config {
     getd("bitmap_cache_fraction", c.bitmap_cache_fraction);
     geti("small_problem_nnz", c.small_problem_nnz);
     geti("spin_wait_us", c.spin_wait_us);
+    geti("force_workflow", c.force_workflow);
+    getd("estimate_scale", c.estimate_scale);
     if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
+    if (c.force_workflow < -1 || c.force_workflow > 2)
+      throw std::invalid_argument("force_workflow must be -1, 0, 1 or 2");
+    if (c.estimate_scale <= 0.0) throw std::invalid_argument("estimate_scale must be positive");
     if (c.bitmap_cache_fraction < 0.0 || c.bitmap_cache_fraction > 0.9)
       throw std::invalid_argument("bitmap_cache_fraction must be in [0, 0.9]");
     if (c.esc_max_products < 0 || c.esc_max_products > 128)

@@ -20,6 +20,10 @@ struct DevWork {
   uint64_t* rowptr64 = nullptr;  // rows+1 exclusive scan of row_nnz
   uint32_t* rowptr32 = nullptr;  // same, truncated to 32 bits
   uint64_t* bm_off = nullptr;    // per row: word offset of its cached bitmap, or ~0
+  uint32_t* est = nullptr;       // estimation workflow: estimated output count per row
+  uint64_t* est_off = nullptr;   // estimation workflow: exclusive scan of est (slots in the temporary output)
+  uint32_t* cnt = nullptr;       // estimation workflow: true output count per row
+  uint32_t* ovf = nullptr;       // estimation workflow: rows that overflowed their estimate
   unsigned long long* bm_cache = nullptr;  // exact column bitmaps saved by the symbolic pass
   uint64_t bm_cache_words = 0;   // capacity of bm_cache (0: no cache)
   DevCounters* ctr = nullptr;
@@ -49,10 +53,40 @@ template <typename RP>
 int launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int num_sms,
                     cudaStream_t s, cudaEvent_t* bin_events, const unsigned* counts = nullptr);
 
-int launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s);
+// Exclusive scan of in[w.rows] into out64 (and out32 if given), total into
+// *total and out[rows]; with bin_rows, also appends every row to its numeric
+// class (chosen from in[] as the output count).
+int launch_scan(const DevWork& w, const uint32_t* in, uint64_t* out64, uint32_t* out32,
+                unsigned long long* total, bool bin_rows, const NumPolicy& pol, cudaStream_t s);
+
+// HLL (estimation workflow): sketches of B's rows (2^log2p one-byte registers
+// each, into `sketch`) and the compaction statistics of the LCG-sampled rows
+// of A (into the counters).
+template <typename RP>
+int launch_hll_sketch_sample(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int log2p, unsigned sample_rows,
+                             uint8_t* sketch, cudaStream_t s);
+
+// Per-row output-size estimates into out[A.rows]: raw HLL union estimates, or
+// (raw = false) the estimate times `expansion`, at least 1 and at most
+// min(products, column span), with the product count for rows of at most
+// esc_max products.
+template <typename RP>
+int launch_hll_rows(const Csr<RP>& A, const DevWork& w, int log2p, double expansion, uint32_t esc_max, bool raw,
+                    const uint8_t* sketch, uint32_t* out, cudaStream_t s);
+
+// Estimation workflow epilogue: copy the rows that fit their estimate from the
+// temporary output into C.
+void launch_copy_rows(const DevWork& w, const uint32_t* t_col, const double* t_val, uint32_t* c_col,
+                      double* c_val, cudaStream_t s);
+
+// Exact counts (bitmap symbolic kernel) and exact numeric output (bitmap
+// numeric kernel) for the rows of the overflow queue.
+template <typename RP>
+int launch_overflow(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, bool numeric, uint32_t* c_col,
+                    double* c_val, int num_sms, cudaStream_t s);
 
 template <typename RP>
-int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_t* c_col,
+int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const OutSpec& out, uint32_t* c_col,
                     double* c_val, int num_sms, cudaStream_t s, cudaEvent_t* bin_events,
                     const unsigned* counts = nullptr);
 

@@ -14,6 +14,7 @@
 // only host read-back of a multiply is the total output count (to allocate C).
 // Numeric kernels write each row already sorted straight into its final place
 // in C, so there is no temporary output buffer and no separate sort/copy pass.
+#include <algorithm>
 #include <cstdio>
 #include "kernels.h"
 
@@ -78,6 +79,22 @@ __device__ __forceinline__ T block_excl_scan(T v, T* scratch, T* total) {
 __device__ __forceinline__ void raise_status(DevCounters* ctr, unsigned bit, uint32_t row) {
   const unsigned old = atomicOr(&ctr->status, bit);
   if (old == 0) ctr->err_row = row;
+}
+
+// One thread per row, once the row's true count n is known: exact mode checks
+// n against the expected count; estimation mode records n and appends the row
+// to the overflow list when it does not fit its slots. Returns whether to write.
+__device__ __forceinline__ bool out_accept(const OutSpec& o, DevCounters* ctr, uint32_t row, uint32_t n,
+                                           uint32_t cap) {
+  if (!o.count) {
+    if (n != cap) raise_status(ctr, DEV_COUNT_MISMATCH, row);
+    return true;
+  }
+  o.count[row] = n;
+  if (n <= cap) return true;
+  const unsigned i = atomicAdd(o.overflow_n, 1u);
+  o.overflow[i] = row;
+  return false;
 }
 
 // Symbolic class of a row from its product count and output column span.
@@ -310,14 +327,13 @@ __device__ __forceinline__ void warp_run_heads(const uint32_t (&key)[K], unsigne
 }
 
 template <typename RP, int K>
-__global__ void __launch_bounds__(256) k_sym_esc(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
-                                                 DevCounters* __restrict__ ctr, int bin,
+__global__ void __launch_bounds__(256) k_sym_esc(Csr<RP> A, Csr<RP> B, RowQueue q, DevCounters* __restrict__ ctr,
                                                  uint32_t* __restrict__ row_nnz) {
   constexpr int CAP = 32 * K;
   __shared__ uint64_t s_src[8][CAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t count = ctr->sym_count[bin];
-  const uint32_t* list = bins + (uint64_t)bin * A.rows;
+  const uint32_t count = *q.count;
+  const uint32_t* list = q.rows;
   for (uint64_t idx = (uint64_t)blockIdx.x * 8 + warp; idx < count; idx += (uint64_t)gridDim.x * 8) {
     const uint32_t row = list[idx];
     const uint32_t np = gather_products<CAP>(A, B, row, s_src[warp], nullptr);
@@ -351,17 +367,15 @@ __global__ void __launch_bounds__(256) k_sym_esc(Csr<RP> A, Csr<RP> B, const uin
 }
 
 template <typename RP, int K>
-__global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
-                                                 DevCounters* __restrict__ ctr, int bin,
-                                                 const uint32_t* __restrict__ row_nnz,
-                                                 const uint64_t* __restrict__ rowptr,
-                                                 uint32_t* __restrict__ c_col, double* __restrict__ c_val) {
+__global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, RowQueue q, OutSpec o,
+                                                 DevCounters* __restrict__ ctr, uint32_t* __restrict__ c_col,
+                                                 double* __restrict__ c_val) {
   constexpr int CAP = 32 * K;
   __shared__ uint64_t s_src[8][CAP];
   __shared__ uint64_t s_aidx[8][CAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t count = ctr->num_count[bin];
-  const uint32_t* list = bins + (uint64_t)bin * A.rows;
+  const uint32_t count = *q.count;
+  const uint32_t* list = q.rows;
   for (uint64_t idx = (uint64_t)blockIdx.x * 8 + warp; idx < count; idx += (uint64_t)gridDim.x * 8) {
     const uint32_t row = list[idx];
     const uint32_t np = gather_products<CAP>(A, B, row, s_src[warp], s_aidx[warp]);
@@ -406,14 +420,17 @@ __global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, const uin
     uint32_t n = 0;
 #pragma unroll
     for (int e = 0; e < K; ++e) n += __popc(hb[e]);
-    const uint32_t expect = row_nnz[row];
-    if (n != expect && lane == 0) raise_status(ctr, DEV_COUNT_MISMATCH, row);
-    const uint64_t off = rowptr[row];
+    const uint32_t cap = o.cap[row];
+    int accept = 0;
+    if (lane == 0) accept = out_accept(o, ctr, row, n, cap);
+    accept = __shfl_sync(kFull, accept, 0);
+    const uint32_t lim = accept ? min(n, cap) : 0u;
+    const uint64_t off = o.off[row];
     uint32_t before = 0;
 #pragma unroll
     for (int e = 0; e < K; ++e) {
       const uint32_t pos = before + __popc(hb[e] & lanemask_lt());
-      if (head[e] && pos < expect) {
+      if (head[e] && pos < lim) {
         c_col[off + pos] = key[e];
         c_val[off + pos] = val[e];
       }
@@ -594,8 +611,7 @@ struct SymHashSmem {
 };
 
 template <typename RP, int NT, int LOG2T>
-__global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
-                                                 DevCounters* __restrict__ ctr, int bin,
+__global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, RowQueue q, DevCounters* __restrict__ ctr,
                                                  const uint32_t* __restrict__ prod,
                                                  uint32_t* __restrict__ row_nnz) {
   constexpr int T = 1 << LOG2T;
@@ -603,10 +619,10 @@ __global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, const uin
   SymHashSmem<NT, LOG2T>& S = *reinterpret_cast<SymHashSmem<NT, LOG2T>*>(smem_raw);
   const int tid = threadIdx.x;
   for (int i = tid; i < T; i += NT) S.keys[i] = kEmpty;
-  const uint32_t count = ctr->sym_count[bin];
-  const uint32_t* list = bins + (uint64_t)bin * A.rows;
+  const uint32_t count = *q.count;
+  const uint32_t* list = q.rows;
   for (;;) {
-    if (tid == 0) S.s_idx = atomicAdd(&ctr->sym_cursor[bin], 1u);
+    if (tid == 0) S.s_idx = atomicAdd(q.cursor, 1u);
     __syncthreads();
     const uint32_t idx = S.s_idx;
     if (idx >= count) break;
@@ -647,15 +663,12 @@ struct NumHashSmem {
   double vals[1 << LOG2T];
   uint32_t keys[1 << LOG2T];  // reused as (1 << LOG2T) / 2 sort keys of 64 bits
   EnumSmem<NT> e;
-  uint32_t s_idx, s_n;
+  uint32_t s_idx, s_n, s_acc;
 };
 
 template <typename RP, int NT, int LOG2T>
-__global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins,
-                                                 DevCounters* __restrict__ ctr, int bin,
-                                                 const uint32_t* __restrict__ prod,
-                                                 const uint32_t* __restrict__ row_nnz,
-                                                 const uint64_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, RowQueue q, OutSpec o,
+                                                 DevCounters* __restrict__ ctr, const uint32_t* __restrict__ prod,
                                                  uint32_t* __restrict__ c_col, double* __restrict__ c_val) {
   constexpr int T = 1 << LOG2T;
   constexpr int PER = T / NT;
@@ -668,11 +681,11 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uin
     S.keys[i] = kEmpty;
     S.vals[i] = 0.0;
   }
-  const uint32_t count = ctr->num_count[bin];
-  const uint32_t* list = bins + (uint64_t)bin * A.rows;
+  const uint32_t count = *q.count;
+  const uint32_t* list = q.rows;
   for (;;) {
     if (tid == 0) {
-      S.s_idx = atomicAdd(&ctr->num_cursor[bin], 1u);
+      S.s_idx = atomicAdd(q.cursor, 1u);
       S.s_n = 0;
     }
     __syncthreads();
@@ -701,7 +714,10 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uin
       }
       full |= probe == T;
     });
-    if (full) raise_status(ctr, DEV_TABLE_FULL, row);
+    // a full table cannot count the row: an error in exact mode, an overflow
+    // with unknown count in estimation mode
+    const int any_full = __syncthreads_or(full);
+    if (any_full && tid == 0 && !o.count) raise_status(ctr, DEV_TABLE_FULL, row);
     // compaction: read this thread's slots, then rewrite the key area as sort keys
     uint32_t mine[PER];
     unsigned cnt = 0;
@@ -742,11 +758,17 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, const uin
         __syncthreads();
       }
     }
-    const uint32_t expect = row_nnz[row];
-    if (tid == 0 && (n != expect || n > CAP)) raise_status(ctr, DEV_COUNT_MISMATCH, row);
-    // rows that overflowed the sort capacity were not compacted: write nothing
-    const uint32_t wn = (n <= CAP) ? min(n, expect) : 0u;
-    const uint64_t off = rowptr[row];
+    const uint32_t cap = o.cap[row];
+    if (tid == 0) {
+      const uint32_t nn = any_full ? kUnknownCount : n;
+      bool acc = out_accept(o, ctr, row, nn, cap);
+      if (!o.count && n > CAP) raise_status(ctr, DEV_COUNT_MISMATCH, row);
+      S.s_acc = acc && n <= CAP && !any_full;
+    }
+    __syncthreads();
+    // rows that overflowed the sort capacity or their slots are not written
+    const uint32_t wn = S.s_acc ? min(n, cap) : 0u;
+    const uint64_t off = o.off[row];
     for (uint32_t i = tid; i < wn; i += NT) {
       const unsigned long long e = sortbuf[i];
       c_col[off + i] = (uint32_t)(e >> 32);
@@ -773,7 +795,7 @@ struct BitmapSymSmem {
 
 template <typename RP>
 __global__ void __launch_bounds__(kBitmapThreads, 1)
-    k_sym_bitmap(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins, DevCounters* __restrict__ ctr,
+    k_sym_bitmap(Csr<RP> A, Csr<RP> B, RowQueue q, DevCounters* __restrict__ ctr,
                  const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
                  const uint32_t* __restrict__ hi, uint32_t* __restrict__ row_nnz, uint64_t* __restrict__ bm_off,
                  unsigned long long* __restrict__ cache, uint64_t cache_words) {
@@ -781,10 +803,10 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
   BitmapSymSmem& S = *reinterpret_cast<BitmapSymSmem*>(smem_raw);
   const int tid = threadIdx.x;
   for (int i = tid; i < kBitmapWords; i += kBitmapThreads) S.bits[i] = 0ull;
-  const uint32_t count = ctr->sym_count[SB_BITMAP];
-  const uint32_t* list = bins + (uint64_t)SB_BITMAP * A.rows;
+  const uint32_t count = *q.count;
+  const uint32_t* list = q.rows;
   for (;;) {
-    if (tid == 0) S.s_idx = atomicAdd(&ctr->sym_cursor[SB_BITMAP], 1u);
+    if (tid == 0) S.s_idx = atomicAdd(q.cursor, 1u);
     __syncthreads();
     const uint32_t idx = S.s_idx;
     if (idx >= count) break;
@@ -837,34 +859,39 @@ struct BitmapNumSmem {
   uint32_t spre[kBitmapWords / 1024];  // popcount of the superblocks before each superblock
   uint32_t scan[33];
   EnumSmem<kBitmapThreads> e;
-  uint32_t s_idx;
+  uint32_t s_idx, s_acc;
 };
 
 template <typename RP>
 __global__ void __launch_bounds__(kBitmapThreads, 1)
-    k_num_bitmap(Csr<RP> A, Csr<RP> B, const uint32_t* __restrict__ bins, DevCounters* __restrict__ ctr,
+    k_num_bitmap(Csr<RP> A, Csr<RP> B, RowQueue q, OutSpec o, DevCounters* __restrict__ ctr,
                  const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
-                 const uint32_t* __restrict__ hi, const uint32_t* __restrict__ row_nnz,
-                 const uint64_t* __restrict__ rowptr, const uint64_t* __restrict__ bm_off,
+                 const uint32_t* __restrict__ hi, const uint64_t* __restrict__ bm_off,
                  const unsigned long long* __restrict__ cache, uint32_t* __restrict__ c_col,
                  double* __restrict__ c_val) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BitmapNumSmem& S = *reinterpret_cast<BitmapNumSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int i = tid; i < kBitmapWords; i += kBitmapThreads) S.bits[i] = 0ull;
-  const uint32_t count = ctr->num_count[NB_BITMAP];
-  const uint32_t* list = bins + (uint64_t)NB_BITMAP * A.rows;
+  const uint32_t count = *q.count;
+  const uint32_t* list = q.rows;
   for (;;) {
-    if (tid == 0) S.s_idx = atomicAdd(&ctr->num_cursor[NB_BITMAP], 1u);
+    if (tid == 0) S.s_idx = atomicAdd(q.cursor, 1u);
     __syncthreads();
     const uint32_t idx = S.s_idx;
     if (idx >= count) break;
     const uint32_t row = list[idx];
     const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
     const uint64_t rlo = lo[row], rhi = hi[row];
-    const uint64_t row_off = rowptr[row];
-    const uint32_t expect = row_nnz[row];
+    const uint64_t row_off = o.off[row];
+    const uint32_t expect = o.cap[row];
     const uint64_t row_lim = row_off + expect;
+    // estimation mode counts a row before writing it; a row wider than one
+    // window is not counted here and goes to the overflow list
+    if (o.count && rhi - rlo + 1 > kBitmapBits) {
+      if (tid == 0) out_accept(o, ctr, row, kUnknownCount, expect);
+      continue;
+    }
     const uint64_t slot = cache ? bm_off[row] : ~0ull;
     uint64_t off = row_off;
     // a row whose A entries fit one chunk is loaded once for both passes
@@ -894,6 +921,22 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       }
       uint32_t nw_total;
       uint32_t run = block_excl_scan<kBitmapThreads, uint32_t>(local, S.scan, &nw_total);
+      if (o.count) {
+        // estimation mode (single window): the count is known now; a row that
+        // does not fit its slots is listed and skipped
+        if (tid == 0) S.s_acc = out_accept(o, ctr, row, nw_total, expect);
+        __syncthreads();
+        if (!S.s_acc) {
+#pragma unroll
+          for (int i = 0; i < kWordsPerThread; ++i) {
+            const uint32_t w = wbeg + i;
+            if (w < nwords) S.bits[w] = 0ull;
+          }
+          __syncthreads();
+          off = row_lim;
+          break;
+        }
+      }
       if ((tid & 63) == 0) S.spre[tid >> 6] = run;
       __syncthreads();
       const uint32_t sp0 = S.spre[tid >> 6];
@@ -968,7 +1011,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       off += nw_total;
       __syncthreads();
     }
-    if (tid == 0 && off != row_lim) raise_status(ctr, DEV_COUNT_MISMATCH, row);
+    if (tid == 0 && !o.count && off != row_lim) raise_status(ctr, DEV_COUNT_MISMATCH, row);
   }
 }
 
@@ -988,7 +1031,7 @@ __global__ void __launch_bounds__(1024) k_scan_reduce(const uint32_t* __restrict
 }
 
 __global__ void __launch_bounds__(1024) k_scan_tiles(unsigned long long* __restrict__ tile_sums,
-                                                     uint64_t ntiles, DevCounters* __restrict__ ctr,
+                                                     uint64_t ntiles, unsigned long long* __restrict__ total_out,
                                                      uint64_t* __restrict__ rowptr64,
                                                      uint32_t* __restrict__ rowptr32, uint64_t rows) {
   __shared__ unsigned long long scr[33];
@@ -1007,9 +1050,9 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(unsigned long long* __restr
     }
   }
   if (threadIdx.x == 0) {
-    ctr->total_nnz = total;
+    *total_out = total;
     rowptr64[rows] = total;
-    rowptr32[rows] = (uint32_t)total;
+    if (rowptr32) rowptr32[rows] = (uint32_t)total;
   }
 }
 
@@ -1025,7 +1068,7 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
                                                      const uint32_t* __restrict__ anz,
                                                      const uint64_t* __restrict__ bm_off,
                                                      uint32_t* __restrict__ num_bins,
-                                                     DevCounters* __restrict__ ctr, NumPolicy pol) {
+                                                     DevCounters* __restrict__ ctr, NumPolicy pol, int bin_rows) {
   __shared__ unsigned long long scr[33];
   __shared__ unsigned long long s_cls[3][NB_COUNT];
   if (threadIdx.x < 3 * NB_COUNT) (&s_cls[0][0])[threadIdx.x] = 0ull;
@@ -1047,8 +1090,10 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
     int b = -1;
     if (i < n) {
       rowptr64[i] = run;
-      rowptr32[i] = (uint32_t)run;
+      if (rowptr32) rowptr32[i] = (uint32_t)run;
       run += v[q];
+    }
+    if (i < n && bin_rows) {
       const uint32_t p = prod[i];
       b = num_bin_for(v[q], p, (uint64_t)hi[i] - lo[i] + 1, pol);
       if (b >= 0 && pol.force_bin < 0 && bm_off[i] != ~0ull) b = NB_BITMAP;  // reuse the saved bitmap
@@ -1061,8 +1106,9 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
         }
       }
     }
-    bin_append(b, (uint32_t)i, ctr->num_count, num_bins, n);
+    if (bin_rows) bin_append(b, (uint32_t)i, ctr->num_count, num_bins, n);
   }
+  if (!bin_rows) return;
   // warp sums first, then one shared atomic per warp and class
   const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -1108,6 +1154,156 @@ __global__ void k_murmur3(const uint32_t* __restrict__ keys, uint32_t* __restric
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x)
     out[i] = murmur3_u32(keys[i], seed);
+}
+
+// ---------------------------------------------------------------- HyperLogLog
+// Row-size estimates (reference: kernels/HLL.cuh:11-357). A B row's sketch has
+// 2^P one-byte registers: register (h & (2^P-1)) keeps the largest
+// clz(h) + 1 (capped at 32 - P + 1) over the MurmurHash3 values h of the row's
+// column ids (seed 1234). The sketch of an A row's output is the register-wise
+// maximum over the sketches of the B rows it references; the estimate is
+// E = alpha_P * m^2 / sum 2^-M[i], replaced by m * ln(m / V) when V registers
+// are empty and E < 2.5 m.
+constexpr uint32_t kMurmurSeed = 1234;
+
+template <typename RP, int LOGP>
+__global__ void __launch_bounds__(256) k_hll_sketch(Csr<RP> B, uint8_t* __restrict__ sk) {
+  constexpr int M = 1 << LOGP;
+  __shared__ unsigned regs[8][M];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint64_t r = (uint64_t)blockIdx.x * 8 + warp; r < B.rows; r += (uint64_t)gridDim.x * 8) {
+    for (int i = lane; i < M; i += 32) regs[warp][i] = 0u;
+    __syncwarp();
+    const uint64_t b1 = B.row_end(r);
+    for (uint64_t q = B.row_begin(r) + lane; q < b1; q += 32) {
+      const uint32_t h = murmur3_u32(B.col[q], kMurmurSeed);
+      unsigned v = (unsigned)__clz(h) + 1u;
+      if (v > 32u - LOGP + 1u) v = 32u - LOGP + 1u;
+      atomicMax(&regs[warp][h & (M - 1)], v);
+    }
+    __syncwarp();
+    for (int i = lane; i < M; i += 32) sk[r * M + i] = (uint8_t)regs[warp][i];
+    __syncwarp();
+  }
+}
+
+// Raw HLL estimate of the output size of A row `row` (warp-collective; every
+// lane gets the result). Lane l merges word (l % W) of the sketches of every
+// (32 / W)-th A entry with a packed per-byte maximum; xor shuffles finish the
+// union; the harmonic sum runs over the lanes that own a word.
+template <typename RP, int LOGP>
+__device__ __forceinline__ int hll_row_estimate(const Csr<RP>& A, const uint8_t* __restrict__ sk, uint64_t row) {
+  constexpr int M = 1 << LOGP;
+  constexpr int W = M / 4;       // 32-bit words per sketch
+  constexpr int G = 32 / W;      // A entries merged per step
+  constexpr double kAlpha = LOGP == 4 ? 0.673 : (LOGP == 5 ? 0.697 : (LOGP == 6 ? 0.709 : 0.715));
+  const int lane = threadIdx.x & 31;
+  const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+  unsigned acc = 0u;
+  for (uint64_t k = a0 + lane / W; k < a1; k += G) {
+    const uint32_t j = A.col[k];
+    acc = __vmaxu4(acc, reinterpret_cast<const unsigned*>(sk + (uint64_t)j * M)[lane % W]);
+  }
+#pragma unroll
+  for (int o = W; o < 32; o <<= 1) acc = __vmaxu4(acc, __shfl_xor_sync(kFull, acc, o));
+  double z = 0.0;
+  int zeros = 0;
+  if (lane < W) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int v = (acc >> (8 * b)) & 0xFF;
+      z += ldexp(1.0, -v);
+      zeros += v == 0;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    z += __shfl_xor_sync(kFull, z, o);
+    zeros += __shfl_xor_sync(kFull, zeros, o);
+  }
+  int result = (int)(kAlpha * M * M / z);
+  if (zeros != 0 && result < 2.5 * M) result = (int)(M * log((double)M / (double)zeros));
+  return result;
+}
+
+// Estimated output count of every A row for the estimation workflow: rows of at
+// most esc_max products get their product count (an exact upper bound, they run
+// in the register classes); others the HLL estimate times `expansion`, at least
+// 1 and at most min(products, column span).
+template <typename RP, int LOGP>
+__global__ void __launch_bounds__(256) k_hll_estimate(Csr<RP> A, const uint8_t* __restrict__ sk,
+                                                      const uint32_t* __restrict__ prod,
+                                                      const uint32_t* __restrict__ lo,
+                                                      const uint32_t* __restrict__ hi, uint32_t* __restrict__ est,
+                                                      double expansion, uint32_t esc_max, int raw_only) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint64_t r = (uint64_t)blockIdx.x * 8 + warp; r < A.rows; r += (uint64_t)gridDim.x * 8) {
+    const uint32_t p = prod[r];
+    if (!raw_only && p <= esc_max) {  // warp-uniform
+      if (lane == 0) est[r] = p;
+      continue;
+    }
+    const int raw = hll_row_estimate<RP, LOGP>(A, sk, r);
+    if (raw_only) {
+      if (lane == 0) est[r] = raw > 0 ? (uint32_t)raw : 0u;
+      continue;
+    }
+    if (lane == 0) {
+      const uint64_t span = (uint64_t)hi[r] - lo[r] + 1;
+      double e = ceil((double)raw * expansion);
+      if (e < 1.0) e = 1.0;
+      uint64_t v = (uint64_t)e;
+      v = v < p ? v : p;
+      v = v < span ? v : span;
+      est[r] = (uint32_t)v;
+    }
+  }
+}
+
+// Compaction statistics of the LCG-sampled rows (reference: kernels/HLL.cuh:239-357;
+// sample i takes row ((1664525 x + 1013904223) mod 2^32) mod rows with
+// x = 112233 + i * 2654435761). Rows without products or with a zero estimate
+// are skipped (their ratio is undefined).
+template <typename RP, int LOGP>
+__global__ void __launch_bounds__(256) k_hll_sample(Csr<RP> A, const uint8_t* __restrict__ sk,
+                                                    const uint32_t* __restrict__ prod, unsigned samples,
+                                                    DevCounters* __restrict__ ctr) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint64_t i = (uint64_t)blockIdx.x * 8 + warp; i < samples; i += (uint64_t)gridDim.x * 8) {
+    uint64_t x = 112233ull + i * 2654435761ull;
+    x = (1664525ull * x + 1013904223ull) % (1ull << 32);
+    const uint64_t row = x % A.rows;
+    const uint32_t p = prod[row];
+    if (p == 0) continue;
+    const int raw = hll_row_estimate<RP, LOGP>(A, sk, row);
+    if (lane == 0 && raw > 0) {
+      atomicAdd(&ctr->sample_rows, 1u);
+      atomicAdd(&ctr->sample_products, (unsigned long long)p);
+      atomicAdd(&ctr->sample_est, (double)raw);
+      atomicAdd(&ctr->sample_compaction, (double)p / (double)raw);
+    }
+  }
+}
+
+// Estimation-workflow epilogue: rows that fit their estimate are copied from
+// the temporary output (slots at src_off) to C (dst_off), one warp per row.
+__global__ void __launch_bounds__(256) k_copy_rows(uint64_t rows, const uint64_t* __restrict__ src_off,
+                                                   const uint32_t* __restrict__ cap,
+                                                   const uint32_t* __restrict__ cnt,
+                                                   const uint64_t* __restrict__ dst_off,
+                                                   const uint32_t* __restrict__ t_col,
+                                                   const double* __restrict__ t_val, uint32_t* __restrict__ c_col,
+                                                   double* __restrict__ c_val) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint64_t r = (uint64_t)blockIdx.x * 8 + warp; r < rows; r += (uint64_t)gridDim.x * 8) {
+    const uint32_t n = cnt[r];
+    if (n == 0 || n == kUnknownCount || n > cap[r]) continue;
+    const uint64_t s0 = src_off[r], d0 = dst_off[r];
+    for (uint32_t i = lane; i < n; i += 32) {
+      c_col[d0 + i] = t_col[s0 + i];
+      c_val[d0 + i] = t_val[s0 + i];
+    }
+  }
 }
 
 // ---------------------------------------------------------------- launchers
@@ -1204,49 +1400,53 @@ int launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int nu
   auto grid = [&](int kind, int cls, unsigned per_block) {
     return class_grid(num_sms, g_occ[kind], counts, cls, per_block);
   };
+  auto queue = [&](int c) {
+    return RowQueue{w.sym_bins + (uint64_t)c * A.rows, w.ctr->sym_count + c, w.ctr->sym_cursor + c};
+  };
   unsigned gsz;
   mark(SB_ESC1);
   if ((gsz = grid(K_SYM_ESC1, SB_ESC1, 8)) && ++launched)
-    k_sym_esc<RP, 1><<<gsz, 256, 0, s>>>(A, B, w.sym_bins, w.ctr, SB_ESC1, w.row_nnz);
+    k_sym_esc<RP, 1><<<gsz, 256, 0, s>>>(A, B, queue(SB_ESC1), w.ctr, w.row_nnz);
   mark(SB_ESC2);
   if ((gsz = grid(K_SYM_ESC2, SB_ESC2, 8)) && ++launched)
-    k_sym_esc<RP, 2><<<gsz, 256, 0, s>>>(A, B, w.sym_bins, w.ctr, SB_ESC2, w.row_nnz);
+    k_sym_esc<RP, 2><<<gsz, 256, 0, s>>>(A, B, queue(SB_ESC2), w.ctr, w.row_nnz);
   mark(SB_ESC4);
   if ((gsz = grid(K_SYM_ESC4, SB_ESC4, 8)) && ++launched)
-    k_sym_esc<RP, 4><<<gsz, 256, 0, s>>>(A, B, w.sym_bins, w.ctr, SB_ESC4, w.row_nnz);
+    k_sym_esc<RP, 4><<<gsz, 256, 0, s>>>(A, B, queue(SB_ESC4), w.ctr, w.row_nnz);
   mark(SB_HASH_S);
   if ((gsz = grid(K_SYM_S, SB_HASH_S, 1)) && ++launched)
-    k_sym_hash<RP, 128, 11><<<gsz, 128, sym_hash_smem<128, 11>(), s>>>(A, B, w.sym_bins, w.ctr, SB_HASH_S, w.prod,
+    k_sym_hash<RP, 128, 11><<<gsz, 128, sym_hash_smem<128, 11>(), s>>>(A, B, queue(SB_HASH_S), w.ctr, w.prod,
                                                                        w.row_nnz);
   mark(SB_HASH_M);
   if ((gsz = grid(K_SYM_M, SB_HASH_M, 1)) && ++launched)
-    k_sym_hash<RP, 256, 13><<<gsz, 256, sym_hash_smem<256, 13>(), s>>>(A, B, w.sym_bins, w.ctr, SB_HASH_M, w.prod,
+    k_sym_hash<RP, 256, 13><<<gsz, 256, sym_hash_smem<256, 13>(), s>>>(A, B, queue(SB_HASH_M), w.ctr, w.prod,
                                                                        w.row_nnz);
   mark(SB_HASH_L);
   if ((gsz = grid(K_SYM_L, SB_HASH_L, 1)) && ++launched)
-    k_sym_hash<RP, 512, 15><<<gsz, 512, sym_hash_smem<512, 15>(), s>>>(A, B, w.sym_bins, w.ctr, SB_HASH_L, w.prod,
+    k_sym_hash<RP, 512, 15><<<gsz, 512, sym_hash_smem<512, 15>(), s>>>(A, B, queue(SB_HASH_L), w.ctr, w.prod,
                                                                        w.row_nnz);
   mark(SB_BITMAP);
   if ((gsz = grid(K_SYM_BM, SB_BITMAP, 1)) && ++launched)
-    k_sym_bitmap<RP><<<gsz, kBitmapThreads, kSymBitmapSmem, s>>>(A, B, w.sym_bins, w.ctr, w.prod, w.lo, w.hi,
+    k_sym_bitmap<RP><<<gsz, kBitmapThreads, kSymBitmapSmem, s>>>(A, B, queue(SB_BITMAP), w.ctr, w.prod, w.lo, w.hi,
                                                                  w.row_nnz, w.bm_off, w.bm_cache, w.bm_cache_words);
   mark(SB_COUNT);
   return launched;
 }
 
-int launch_scan(const DevWork& w, const NumPolicy& pol, cudaStream_t s) {
+int launch_scan(const DevWork& w, const uint32_t* in, uint64_t* out64, uint32_t* out32,
+                unsigned long long* total, bool bin_rows, const NumPolicy& pol, cudaStream_t s) {
   const uint64_t nt = scan_tiles(w.rows);
   if (w.rows == 0) return 0;
-  k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums);
-  k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, w.ctr, w.rowptr64, w.rowptr32, w.rows);
-  k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(w.row_nnz, w.rows, w.tile_sums, w.rowptr64, w.rowptr32,
-                                             w.prod, w.lo, w.hi, w.anz, w.bm_off, w.num_bins, w.ctr, pol);
+  k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(in, w.rows, w.tile_sums);
+  k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, total, out64, out32, w.rows);
+  k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(in, w.rows, w.tile_sums, out64, out32, w.prod, w.lo, w.hi, w.anz,
+                                             w.bm_off, w.num_bins, w.ctr, pol, bin_rows ? 1 : 0);
   return 3;
 }
 
 template <typename RP>
-int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_t* c_col, double* c_val,
-                   int num_sms, cudaStream_t s, cudaEvent_t* ev, const unsigned* counts) {
+int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const OutSpec& o, uint32_t* c_col,
+                   double* c_val, int num_sms, cudaStream_t s, cudaEvent_t* ev, const unsigned* counts) {
   if (A.rows == 0) return 0;
   int launched = 0;
   auto mark = [&](int i) {
@@ -1255,33 +1455,35 @@ int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, uint32_
   auto grid = [&](int kind, int cls, unsigned per_block) {
     return class_grid(num_sms, g_occ[kind], counts, cls, per_block);
   };
+  auto queue = [&](int c) {
+    return RowQueue{w.num_bins + (uint64_t)c * A.rows, w.ctr->num_count + c, w.ctr->num_cursor + c};
+  };
   unsigned gsz;
   mark(NB_ESC1);
   if ((gsz = grid(K_NUM_ESC1, NB_ESC1, 8)) && ++launched)
-    k_num_esc<RP, 1><<<gsz, 256, 0, s>>>(A, B, w.num_bins, w.ctr, NB_ESC1, w.row_nnz, w.rowptr64, c_col, c_val);
+    k_num_esc<RP, 1><<<gsz, 256, 0, s>>>(A, B, queue(NB_ESC1), o, w.ctr, c_col, c_val);
   mark(NB_ESC2);
   if ((gsz = grid(K_NUM_ESC2, NB_ESC2, 8)) && ++launched)
-    k_num_esc<RP, 2><<<gsz, 256, 0, s>>>(A, B, w.num_bins, w.ctr, NB_ESC2, w.row_nnz, w.rowptr64, c_col, c_val);
+    k_num_esc<RP, 2><<<gsz, 256, 0, s>>>(A, B, queue(NB_ESC2), o, w.ctr, c_col, c_val);
   mark(NB_ESC4);
   if ((gsz = grid(K_NUM_ESC4, NB_ESC4, 8)) && ++launched)
-    k_num_esc<RP, 4><<<gsz, 256, 0, s>>>(A, B, w.num_bins, w.ctr, NB_ESC4, w.row_nnz, w.rowptr64, c_col, c_val);
+    k_num_esc<RP, 4><<<gsz, 256, 0, s>>>(A, B, queue(NB_ESC4), o, w.ctr, c_col, c_val);
   mark(NB_HASH_S);
   if ((gsz = grid(K_NUM_S, NB_HASH_S, 1)) && ++launched)
-    k_num_hash<RP, 128, 10><<<gsz, 128, num_hash_smem<128, 10>(), s>>>(A, B, w.num_bins, w.ctr, NB_HASH_S, w.prod,
-                                                                       w.row_nnz, w.rowptr64, c_col, c_val);
+    k_num_hash<RP, 128, 10><<<gsz, 128, num_hash_smem<128, 10>(), s>>>(A, B, queue(NB_HASH_S), o, w.ctr, w.prod,
+                                                                       c_col, c_val);
   mark(NB_HASH_M);
   if ((gsz = grid(K_NUM_M, NB_HASH_M, 1)) && ++launched)
-    k_num_hash<RP, 256, 12><<<gsz, 256, num_hash_smem<256, 12>(), s>>>(A, B, w.num_bins, w.ctr, NB_HASH_M, w.prod,
-                                                                       w.row_nnz, w.rowptr64, c_col, c_val);
+    k_num_hash<RP, 256, 12><<<gsz, 256, num_hash_smem<256, 12>(), s>>>(A, B, queue(NB_HASH_M), o, w.ctr, w.prod,
+                                                                       c_col, c_val);
   mark(NB_HASH_L);
   if ((gsz = grid(K_NUM_L, NB_HASH_L, 1)) && ++launched)
-    k_num_hash<RP, 512, 13><<<gsz, 512, num_hash_smem<512, 13>(), s>>>(A, B, w.num_bins, w.ctr, NB_HASH_L, w.prod,
-                                                                       w.row_nnz, w.rowptr64, c_col, c_val);
+    k_num_hash<RP, 512, 13><<<gsz, 512, num_hash_smem<512, 13>(), s>>>(A, B, queue(NB_HASH_L), o, w.ctr, w.prod,
+                                                                       c_col, c_val);
   mark(NB_BITMAP);
   if ((gsz = grid(K_NUM_BM, NB_BITMAP, 1)) && ++launched)
-    k_num_bitmap<RP><<<gsz, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, w.num_bins, w.ctr, w.prod, w.lo, w.hi,
-                                                                 w.row_nnz, w.rowptr64, w.bm_off, w.bm_cache, c_col,
-                                                                 c_val);
+    k_num_bitmap<RP><<<gsz, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, queue(NB_BITMAP), o, w.ctr, w.prod, w.lo,
+                                                                 w.hi, w.bm_off, w.bm_cache, c_col, c_val);
   mark(NB_COUNT);
   return launched;
 }
@@ -1292,6 +1494,69 @@ void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t se
   k_murmur3<<<(unsigned)(blocks > 4096 ? 4096 : blocks), 256, 0, s>>>(keys, out, n, seed);
 }
 
+template <typename RP>
+int launch_hll_sketch_sample(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int log2p, unsigned sample_rows,
+                             uint8_t* sketch, cudaStream_t s) {
+  if (A.rows == 0) return 0;
+  const unsigned gb = (unsigned)std::min<uint64_t>((B.rows + 7) / 8, 65535u * 8);
+  const unsigned gs = (sample_rows + 7) / 8;
+  int n = 0;
+  if (log2p == 5) {
+    if (B.rows) k_hll_sketch<RP, 5><<<gb, 256, 0, s>>>(B, sketch), ++n;
+    if (gs) k_hll_sample<RP, 5><<<gs, 256, 0, s>>>(A, sketch, w.prod, sample_rows, w.ctr), ++n;
+  } else {
+    if (B.rows) k_hll_sketch<RP, 6><<<gb, 256, 0, s>>>(B, sketch), ++n;
+    if (gs) k_hll_sample<RP, 6><<<gs, 256, 0, s>>>(A, sketch, w.prod, sample_rows, w.ctr), ++n;
+  }
+  return n;
+}
+
+template <typename RP>
+int launch_hll_rows(const Csr<RP>& A, const DevWork& w, int log2p, double expansion, uint32_t esc_max, bool raw,
+                    const uint8_t* sketch, uint32_t* out, cudaStream_t s) {
+  if (A.rows == 0) return 0;
+  const unsigned ga = (unsigned)std::min<uint64_t>((A.rows + 7) / 8, 65535u * 8);
+  if (log2p == 5)
+    k_hll_estimate<RP, 5><<<ga, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, raw ? 1 : 0);
+  else
+    k_hll_estimate<RP, 6><<<ga, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, raw ? 1 : 0);
+  return 1;
+}
+
+void launch_copy_rows(const DevWork& w, const uint32_t* t_col, const double* t_val, uint32_t* c_col, double* c_val,
+                      cudaStream_t s) {
+  if (w.rows == 0) return;
+  const unsigned g = (unsigned)std::min<uint64_t>((w.rows + 7) / 8, 148u * 64u);
+  k_copy_rows<<<g, 256, 0, s>>>(w.rows, w.est_off, w.est, w.cnt, w.rowptr64, t_col, t_val, c_col, c_val);
+}
+
+template <typename RP>
+int launch_overflow(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, bool numeric, uint32_t* c_col,
+                    double* c_val, int num_sms, cudaStream_t s) {
+  const RowQueue q{w.ovf, &w.ctr->overflow_n, w.ctr->overflow_cursor + (numeric ? 1 : 0)};
+  if (!numeric) {
+    k_sym_bitmap<RP><<<num_sms, kBitmapThreads, kSymBitmapSmem, s>>>(A, B, q, w.ctr, w.prod, w.lo, w.hi, w.cnt,
+                                                                     w.bm_off, nullptr, 0);
+  } else {
+    const OutSpec o{w.rowptr64, w.cnt, nullptr, nullptr, nullptr};
+    k_num_bitmap<RP><<<num_sms, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, q, o, w.ctr, w.prod, w.lo, w.hi, w.bm_off,
+                                                                     nullptr, c_col, c_val);
+  }
+  return 1;
+}
+
+template int launch_hll_sketch_sample<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, int,
+                                                unsigned, uint8_t*, cudaStream_t);
+template int launch_hll_sketch_sample<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, int,
+                                                unsigned, uint8_t*, cudaStream_t);
+template int launch_hll_rows<uint32_t>(const Csr<uint32_t>&, const DevWork&, int, double, uint32_t, bool,
+                                       const uint8_t*, uint32_t*, cudaStream_t);
+template int launch_hll_rows<uint64_t>(const Csr<uint64_t>&, const DevWork&, int, double, uint32_t, bool,
+                                       const uint8_t*, uint32_t*, cudaStream_t);
+template int launch_overflow<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, bool, uint32_t*,
+                                       double*, int, cudaStream_t);
+template int launch_overflow<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, bool, uint32_t*,
+                                       double*, int, cudaStream_t);
 template int launch_analysis<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
                                         const SymPolicy&, cudaStream_t);
 template int launch_analysis<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
@@ -1300,9 +1565,9 @@ template int launch_symbolic<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>
                                         cudaStream_t, cudaEvent_t*, const unsigned*);
 template int launch_symbolic<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, int,
                                         cudaStream_t, cudaEvent_t*, const unsigned*);
-template int launch_numeric<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
-                                       uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*);
-template int launch_numeric<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
-                                       uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*);
+template int launch_numeric<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, const OutSpec&,
+                                      uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*);
+template int launch_numeric<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, const OutSpec&,
+                                      uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*);
 
 }  // namespace ocean

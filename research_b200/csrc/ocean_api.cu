@@ -83,6 +83,10 @@ struct Stats {
   uint64_t cache_words = 0, cache_used = 0;
   bool cache_dropped = false;
   int launches = 0;  // kernels launched by the last call
+  uint64_t total_est = 0, overflow_rows = 0;
+  int hll_log2p = 0;
+  double hll_expansion = 0.0, compaction1 = 0.0, compaction2 = 0.0;
+  bool sampled = false;
   int workflow = 0;  // 0 = precise (symbolic + numeric)
   int rowptr_bits = 32;
   bool valid = false;
@@ -156,7 +160,7 @@ struct ocean_handle {
   void free_all() {
     DevWork& x = w;
     void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
-                  x.rowptr32, x.bm_off, x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
+                  x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf, x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
     for (void* p : ps)
       if (p) cudaFree(p);
     if (h_ctr) cudaFreeHost(h_ctr);
@@ -198,7 +202,7 @@ void ensure_rows(ocean_handle* h, uint64_t rows) {
   }
   DevWork& x = h->w;
   void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32,
-                x.bm_off};
+                x.bm_off, x.est, x.est_off, x.cnt, x.ovf};
   for (void* p : ps)
     if (p) cudaFree(p);
   const uint64_t r = std::max<uint64_t>(rows, 1);
@@ -213,6 +217,10 @@ void ensure_rows(ocean_handle* h, uint64_t rows) {
   OCEAN_CUDA(cudaMalloc((void**)&x.rowptr64, (r + 1) * 8));
   OCEAN_CUDA(cudaMalloc((void**)&x.rowptr32, (r + 1) * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.bm_off, r * 8));
+  OCEAN_CUDA(cudaMalloc((void**)&x.est, r * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.est_off, (r + 1) * 8));
+  OCEAN_CUDA(cudaMalloc((void**)&x.cnt, r * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.ovf, r * 4));
   h->cap_rows = r;
   x.rows = rows;
 }
@@ -274,8 +282,6 @@ Csr<RP> to_csr(const ocean_csr_view* m, const RP* rp) {
   return c;
 }
 
-// Runs analysis + symbolic + scan. Leaves exact per-row counts in w.row_nnz,
-// row pointers in w.rowptr64/32 and the counters in h->h_ctr (read back).
 // Bytes the device could still hand out: free memory plus what the stream-ordered
 // pool holds in reserve.
 uint64_t available_device_bytes(int device) {
@@ -290,39 +296,51 @@ uint64_t available_device_bytes(int device) {
   return (uint64_t)free_b + (reserved > used ? reserved - used : 0);
 }
 
-// Runs analysis + symbolic + scan. Leaves exact per-row counts in w.row_nnz,
-// row pointers in w.rowptr64/32 and the counters in h->h_ctr (read back).
-// With allow_cache, the symbolic pass saves the bitmaps of single-window
-// bitmap-class rows into h->w.bm_cache (allocated here on `s`, sized from the
-// analysis read-back and capped by bitmap_cache_fraction of free memory).
+// Policies of the class choice from the config.
+void make_policies(const Config& c, SymPolicy* sp, NumPolicy* np) {
+  sp->esc_max_products = (uint32_t)c.esc_max_products;
+  sp->force_bin = c.force_sym_bin;
+  np->esc_max_products = (uint32_t)c.esc_max_products;
+  np->force_bin = c.force_num_bin;
+  OCEAN_CHECK(sp->force_bin < SB_COUNT && np->force_bin < NB_COUNT, OCEAN_ERR_INVALID, "forced class out of range");
+}
+
+// Phase 1: row analysis. Large inputs read the counters back (class sizes,
+// product totals); small inputs skip the read-back. Returns whether it read back.
 template <typename RP>
-void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool with_scan,
-               bool allow_cache) {
+bool run_analysis(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s) {
   ensure_rows(h, A.rows);
   OCEAN_CUDA(cudaMemsetAsync(h->w.ctr, 0, sizeof(DevCounters), s));
   SymPolicy sp;
-  sp.esc_max_products = (uint32_t)h->cfg.esc_max_products;
-  sp.force_bin = h->cfg.force_sym_bin;
   NumPolicy np;
-  np.esc_max_products = (uint32_t)h->cfg.esc_max_products;
-  np.force_bin = h->cfg.force_num_bin;
-  OCEAN_CHECK(sp.force_bin < SB_COUNT && np.force_bin < NB_COUNT, OCEAN_ERR_INVALID, "forced class out of range");
+  make_policies(h->cfg, &sp, &np);
   h->w.bm_cache = nullptr;
   h->w.bm_cache_words = 0;
   record(h, EV_START, s);
   h->st.launches = launch_analysis(A, B, h->w, sp, s);
   OCEAN_CUDA(cudaGetLastError());
   if (h->cfg.track_stage_times) record(h, EV_ANALYSIS, s);
-  // The class sizes decide which class kernels run and how big the bitmap cache
-  // is. Small inputs skip this read-back: every class kernel is launched (empty
-  // ones exit at once) and no bitmaps are saved.
   const bool readback = A.nnz > (uint64_t)h->cfg.small_problem_nnz;
-  unsigned sym_counts[SB_COUNT];
   if (readback) {
     OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
     OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
-    for (int i = 0; i < SB_COUNT; ++i) sym_counts[i] = h->h_ctr->sym_count[i];
   }
+  return readback;
+}
+
+// Phase 2 of the precise workflow: symbolic class kernels (exact counts into
+// w.row_nnz) and, with_scan, the row-pointer scan and numeric class lists; the
+// counters are read back at the end. With allow_cache (and the class sizes of
+// a read-back), bitmap-class rows save their bitmaps into h->w.bm_cache, whose
+// size comes from the analysis and is capped by bitmap_cache_fraction of free memory.
+template <typename RP>
+void run_symbolic(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool readback,
+                  bool with_scan, bool allow_cache) {
+  SymPolicy sp;
+  NumPolicy np;
+  make_policies(h->cfg, &sp, &np);
+  unsigned sym_counts[SB_COUNT];
+  for (int i = 0; i < SB_COUNT; ++i) sym_counts[i] = h->h_ctr->sym_count[i];
   if (readback && allow_cache && h->cfg.bitmap_cache_fraction > 0.0) {
     const uint64_t want = h->h_ctr->sym_words;
     const uint64_t budget =
@@ -352,13 +370,21 @@ void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t
                                     readback ? sym_counts : nullptr);
   OCEAN_CUDA(cudaGetLastError());
   if (with_scan) {
-    h->st.launches += launch_scan(h->w, np, s);
+    h->st.launches += launch_scan(h->w, h->w.row_nnz, h->w.rowptr64, h->w.rowptr32, &h->w.ctr->total_nnz, true, np, s);
     OCEAN_CUDA(cudaGetLastError());
   }
-  if (h->cfg.track_stage_times) record(h, EV_SCAN, s);
+  if (track) record(h, EV_SCAN, s);
   OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
   OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
   check_device_status(h);
+}
+
+// Analysis + symbolic + scan (ocean_symbolic and the precise workflow).
+template <typename RP>
+void run_front(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool with_scan,
+               bool allow_cache) {
+  const bool readback = run_analysis(h, A, B, s);
+  run_symbolic(h, A, B, s, readback, with_scan, allow_cache);
 }
 
 // Stops using the saved bitmaps for this call (the buffer stays with the handle).
@@ -378,6 +404,96 @@ void drop_cache_buffer(ocean_handle* h, cudaStream_t s) {
   h->cache_cap_words = 0;
 }
 
+// Workflow ids as reported in the stats (reference: kernels/SpGEMM.cuh:1807-1817).
+enum Workflow { WF_PRECISE = 0, WF_ESTIMATION = 1, WF_ULTRASPARSE = 2 };
+
+// Chooses the workflow after the analysis (reference rules,
+// kernels/SpGEMM.cuh:456-540 and kernels/Analysis.cuh:10-29):
+//  * ultra-sparse when the mean row has at most usparse_avg_product_threshold
+//    products: every row's estimate is its product count (never overflows);
+//  * estimation when products / nnz(A) reaches estimation_input_expansion_threshold
+//    and the HLL-sampled compaction (products per estimated output) reaches
+//    estimation_output_compaction_threshold twice (sum ratio and mean ratio);
+//  * precise otherwise, for small inputs (no read-back), or when the temporary
+//    output of an estimated workflow would not fit in memory.
+// For the estimation workflow the HLL estimates are left in w.est.
+template <typename RP>
+int choose_workflow(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool readback) {
+  const Config& c = h->cfg;
+  if (c.force_workflow == WF_PRECISE || (!readback && c.force_workflow < 0)) return WF_PRECISE;
+  const DevCounters& k = *h->h_ctr;
+  const uint64_t products = readback ? k.total_products : 0;
+  if (c.force_workflow == WF_ULTRASPARSE ||
+      (c.force_workflow < 0 && c.use_ultrasparse_workflow && A.rows &&
+       (double)products / (double)A.rows <= c.usparse_avg_product_threshold &&
+       12.0 * (double)products < 0.4 * (double)available_device_bytes(h->device))) {
+    OCEAN_CUDA(cudaMemcpyAsync(h->w.est, h->w.prod, A.rows * 4, cudaMemcpyDeviceToDevice, s));
+    return WF_ULTRASPARSE;
+  }
+  if (c.force_workflow < 0) {
+    if (!c.use_estimation_workflow) return WF_PRECISE;
+    if (A.nnz == 0 || products / A.nnz < (uint64_t)c.estimation_input_expansion_threshold) return WF_PRECISE;
+  }
+  // HLL estimates and sampled compaction
+  const uint64_t ratio = A.nnz ? products / A.nnz : 0;
+  const int log2p = (readback && ratio >= (uint64_t)c.hll_higher_precision_expansion_threshold) ? 6 : 5;
+  const double expansion = (log2p == 5 ? 2.0 : 1.5) * c.estimate_scale;
+  int samples = (int)(A.rows * c.hll_sample_rate);
+  samples = std::max(samples, c.hll_sample_min_rows);
+  samples = std::min(samples, c.hll_sample_max_rows);
+  void* sk = nullptr;
+  OCEAN_CUDA(cudaMallocAsync(&sk, std::max<uint64_t>(B.rows, 1) << log2p, s));
+  int wf = WF_ESTIMATION;
+  try {
+    h->st.launches += launch_hll_sketch_sample(A, B, h->w, log2p, (unsigned)samples, (uint8_t*)sk, s);
+    OCEAN_CUDA(cudaGetLastError());
+    OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+    OCEAN_CUDA(wait_stream(s, c.spin_wait_us));
+    h->st.hll_log2p = log2p;
+    h->st.hll_expansion = expansion;
+    const unsigned n = h->h_ctr->sample_rows;
+    h->st.compaction1 = n && h->h_ctr->sample_est > 0 ? (double)h->h_ctr->sample_products / h->h_ctr->sample_est : 0.0;
+    h->st.compaction2 = n ? h->h_ctr->sample_compaction / n : 0.0;
+    h->st.sampled = true;
+    if (c.force_workflow != WF_ESTIMATION && (h->st.compaction1 < c.estimation_output_compaction_threshold ||
+                                              h->st.compaction2 < c.estimation_output_compaction_threshold))
+      wf = WF_PRECISE;
+    if (wf == WF_ESTIMATION) {
+      h->st.launches += launch_hll_rows(A, h->w, log2p, expansion, (uint32_t)c.esc_max_products, false,
+                                        (const uint8_t*)sk, h->w.est, s);
+      OCEAN_CUDA(cudaGetLastError());
+    }
+  } catch (...) {
+    cudaFreeAsync(sk, s);
+    throw;
+  }
+  cudaFreeAsync(sk, s);
+  return wf;
+}
+
+// C's buffers; if they do not fit and bitmaps are saved, the bitmaps are
+// dropped (the numeric pass then marks its columns itself) and C retried.
+void alloc_c(ocean_handle* h, CResult* owner, uint64_t rows, uint64_t nnz, int bits, cudaStream_t s) {
+  auto attempt = [&]() -> cudaError_t {
+    cudaError_t e = cudaMallocAsync(&owner->rowptr, (rows + 1) * (bits / 8), s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&owner->col, std::max<uint64_t>(nnz, 1) * 4, s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&owner->val, std::max<uint64_t>(nnz, 1) * 8, s);
+    return e;
+  };
+  cudaError_t e = attempt();
+  if (e != cudaSuccess && h->w.bm_cache) {
+    cudaGetLastError();
+    for (void** p : {&owner->rowptr, (void**)&owner->col, (void**)&owner->val}) {
+      if (*p) cudaFreeAsync(*p, s);
+      *p = nullptr;
+    }
+    drop_cache_buffer(h, s);
+    h->st.cache_dropped = true;
+    e = attempt();
+  }
+  OCEAN_CUDA(e);
+}
+
 template <typename RP>
 void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view* Bv, const RP* arp,
                 const RP* brp, ocean_csr* C, cudaStream_t s) {
@@ -389,51 +505,80 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   st.a_rows = A.rows, st.a_cols = A.cols, st.a_nnz = A.nnz;
   st.b_rows = B.rows, st.b_cols = B.cols, st.b_nnz = B.nnz;
   h->ev_recorded = false;
+  const bool track = h->cfg.track_stage_times;
+  NumPolicy np;
+  {
+    SymPolicy sp;
+    make_policies(h->cfg, &sp, &np);
+  }
 
   uint64_t nnz = 0;
-  if (A.rows > 0) {
-    try {
-      run_front(h, A, B, s, true, true);
-    } catch (...) {
-      release_cache(h, s);
-      throw;
-    }
-    nnz = h->h_ctr->total_nnz;
-  } else {
-    std::memset(h->h_ctr, 0, sizeof(DevCounters));
-  }
-  int bits = h->cfg.output_rowptr_bits ? h->cfg.output_rowptr_bits : (nnz >= (1ull << 32) ? 64 : 32);
-  OCEAN_CHECK(!(bits == 32 && nnz >= (1ull << 32)), OCEAN_ERR_INVALID,
-              "nnz(C) >= 2^32 does not fit 32-bit row pointers (output_rowptr_bits=32)");
-  st.cache_words = h->w.bm_cache_words;
-  st.cache_used = std::min<uint64_t>(h->h_ctr->cache_cursor, h->w.bm_cache_words);
+  int wf = WF_PRECISE;
+  void* t_col = nullptr;  // temporary output of the estimated workflows
+  void* t_val = nullptr;
   CResult* owner = new CResult{0};
   try {
-    // C is allocated after the saved bitmaps; if it does not fit, the bitmaps
-    // are dropped (the numeric pass then marks its columns itself) and C retried.
-    auto alloc_c = [&]() -> cudaError_t {
-      cudaError_t e = cudaMallocAsync(&owner->rowptr, (A.rows + 1) * (bits / 8), s);
-      if (e == cudaSuccess) e = cudaMallocAsync((void**)&owner->col, std::max<uint64_t>(nnz, 1) * 4, s);
-      if (e == cudaSuccess) e = cudaMallocAsync((void**)&owner->val, std::max<uint64_t>(nnz, 1) * 8, s);
-      return e;
-    };
-    cudaError_t e = alloc_c();
-    if (e != cudaSuccess && h->w.bm_cache) {
-      cudaGetLastError();
-      for (void** p : {&owner->rowptr, (void**)&owner->col, (void**)&owner->val}) {
-        if (*p) cudaFreeAsync(*p, s);
-        *p = nullptr;
-      }
-      drop_cache_buffer(h, s);
-      st.cache_dropped = true;
-      e = alloc_c();
-    }
-    OCEAN_CUDA(e);
     if (A.rows > 0) {
-      unsigned num_counts[NB_COUNT];
-      for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
-      st.launches += launch_numeric(A, B, h->w, owner->col, owner->val, h->num_sms, s,
-                                    h->cfg.track_stage_times ? h->ev + EV_NUM0 : nullptr, num_counts);
+      const bool readback = run_analysis(h, A, B, s);
+      wf = choose_workflow(h, A, B, s, readback);
+      if (wf == WF_ESTIMATION || wf == WF_ULTRASPARSE) {
+        // scan of the estimates: temporary slots per row, numeric classes by estimate
+        st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s);
+        OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+        OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
+        st.total_est = h->h_ctr->total_est;
+        if (12.0 * (double)st.total_est > 0.45 * (double)available_device_bytes(h->device)) {
+          wf = WF_PRECISE;  // the temporary output would not fit: count exactly instead
+          OCEAN_CUDA(cudaMemsetAsync(h->w.ctr->num_count, 0, sizeof(unsigned) * NB_COUNT * 2, s));
+        }
+      }
+      if (wf == WF_PRECISE) {
+        run_symbolic(h, A, B, s, readback, true, true);
+        nnz = h->h_ctr->total_nnz;
+      } else {
+        OCEAN_CUDA(cudaMallocAsync(&t_col, std::max<uint64_t>(st.total_est, 1) * 4, s));
+        OCEAN_CUDA(cudaMallocAsync(&t_val, std::max<uint64_t>(st.total_est, 1) * 8, s));
+        OCEAN_CUDA(cudaMemsetAsync(h->w.cnt, 0, A.rows * 4, s));
+        unsigned num_counts[NB_COUNT];
+        for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
+        const OutSpec est_out{h->w.est_off, h->w.est, h->w.cnt, h->w.ovf, &h->w.ctr->overflow_n};
+        st.launches += launch_numeric(A, B, h->w, est_out, (uint32_t*)t_col, (double*)t_val, h->num_sms, s,
+                                      track ? h->ev + EV_NUM0 : nullptr, num_counts);
+        // rows that did not fit their estimate: exact counts, then the row pointers
+        st.launches += launch_overflow(A, B, h->w, false, nullptr, nullptr, h->num_sms, s);
+        st.launches += launch_scan(h->w, h->w.cnt, h->w.rowptr64, h->w.rowptr32, &h->w.ctr->total_nnz, false, np, s);
+        OCEAN_CUDA(cudaGetLastError());
+        OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+        OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
+        check_device_status(h);
+        nnz = h->h_ctr->total_nnz;
+        st.overflow_rows = h->h_ctr->overflow_n;
+      }
+    } else {
+      std::memset(h->h_ctr, 0, sizeof(DevCounters));
+    }
+    const int bits = h->cfg.output_rowptr_bits ? h->cfg.output_rowptr_bits : (nnz >= (1ull << 32) ? 64 : 32);
+    OCEAN_CHECK(!(bits == 32 && nnz >= (1ull << 32)), OCEAN_ERR_INVALID,
+                "nnz(C) >= 2^32 does not fit 32-bit row pointers (output_rowptr_bits=32)");
+    st.rowptr_bits = bits;
+    st.cache_words = h->w.bm_cache_words;
+    st.cache_used = std::min<uint64_t>(h->h_ctr->cache_cursor, h->w.bm_cache_words);
+    alloc_c(h, owner, A.rows, nnz, bits, s);
+    if (A.rows > 0) {
+      if (wf == WF_PRECISE) {
+        unsigned num_counts[NB_COUNT];
+        for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
+        const OutSpec exact{h->w.rowptr64, h->w.row_nnz, nullptr, nullptr, nullptr};
+        st.launches += launch_numeric(A, B, h->w, exact, owner->col, owner->val, h->num_sms, s,
+                                      track ? h->ev + EV_NUM0 : nullptr, num_counts);
+      } else {
+        launch_copy_rows(h->w, (const uint32_t*)t_col, (const double*)t_val, owner->col, owner->val, s);
+        st.launches += 1;
+        if (st.overflow_rows) st.launches += launch_overflow(A, B, h->w, true, owner->col, owner->val, h->num_sms, s);
+        cudaFreeAsync(t_col, s);
+        cudaFreeAsync(t_val, s);
+        t_col = t_val = nullptr;
+      }
       OCEAN_CUDA(cudaGetLastError());
       OCEAN_CUDA(cudaMemcpyAsync(owner->rowptr, bits == 64 ? (void*)h->w.rowptr64 : (void*)h->w.rowptr32,
                                  (A.rows + 1) * (bits / 8), cudaMemcpyDeviceToDevice, s));
@@ -444,7 +589,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     release_cache(h, s);
     record(h, EV_END, s);
     h->ev_recorded = true;
-    h->tracked = h->cfg.track_stage_times;
+    h->tracked = track;
     if (h->cfg.sync_on_return && A.rows > 0) {
       OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
       OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
@@ -452,6 +597,8 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     }
   } catch (...) {
     release_cache(h, s);
+    if (t_col) cudaFreeAsync(t_col, s);
+    if (t_val) cudaFreeAsync(t_val, s);
     if (owner->rowptr) cudaFreeAsync(owner->rowptr, s);
     if (owner->col) cudaFreeAsync(owner->col, s);
     if (owner->val) cudaFreeAsync(owner->val, s);
@@ -462,7 +609,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   C->cols = B.cols;
   C->nnz = nnz;
   C->rowptr = owner->rowptr;
-  C->rowptr_bits = bits;
+  C->rowptr_bits = st.rowptr_bits;
   C->col = owner->col;
   C->val = owner->val;
   C->location = 0;
@@ -483,8 +630,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     st.sym_anz[i] = h->h_ctr->sym_anz[i];
     st.sym_prod[i] = h->h_ctr->sym_prod[i];
   }
-  st.rowptr_bits = bits;
-  st.workflow = 0;
+  st.workflow = wf;
   st.valid = true;
   st.host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -548,6 +694,12 @@ std::string stats_json(ocean_handle* h) {
     << ", \"bitmap_cache_bytes\": " << 8 * st.cache_words << ", \"bitmap_cache_used_bytes\": " << 8 * st.cache_used
     << ", \"bitmap_cache_dropped\": " << (st.cache_dropped ? "true" : "false")
     << ", \"kernel_launches\": " << st.launches << "}, ";
+  if (st.sampled)
+    o << "\"sampling\": {\"compaction_1\": " << st.compaction1 << ", \"compaction_2\": " << st.compaction2
+      << "}, ";
+  if (st.workflow == 1 || st.workflow == 2)
+    o << "\"estimation\": {\"overflow_rows\": " << st.overflow_rows << ", \"log2_precision\": " << st.hll_log2p
+      << ", \"total_est\": " << st.total_est << ", \"expansion\": " << st.hll_expansion << "}, ";
   o << "\"binning_1\": [";
   for (int i = 0; i < SB_COUNT; ++i) o << (i ? ", " : "") << st.sym_bins[i];
   o << "], \"binning_2\": [";
@@ -790,6 +942,37 @@ int ocean_symbolic(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_vie
     }
     OCEAN_CUDA(cudaMemcpyAsync(row_nnz, h->w.row_nnz, A->rows * 4, cudaMemcpyDeviceToDevice, s));
     OCEAN_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int ocean_row_estimates(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, int log2p,
+                        uint32_t* est, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    validate_view(A, "A");
+    validate_view(B, "B");
+    OCEAN_CHECK(A->cols == B->rows, OCEAN_ERR_INVALID, "Incompatible matrix dimensions (A.cols != B.rows)");
+    OCEAN_CHECK(A->rowptr_bits == B->rowptr_bits, OCEAN_ERR_INVALID,
+                "ocean_row_estimates needs equal row-pointer widths for A and B");
+    OCEAN_CHECK(log2p == 5 || log2p == 6, OCEAN_ERR_INVALID, "log2p must be 5 or 6");
+    OCEAN_CHECK(A->rows == 0 || est != nullptr, OCEAN_ERR_INVALID, "est is NULL");
+    if (A->rows == 0) return;
+    cudaStream_t s = (cudaStream_t)stream;
+    auto go = [&](auto rp_tag) {
+      using RP = decltype(rp_tag);
+      const Csr<RP> a = to_csr<RP>(A, (const RP*)A->rowptr), b = to_csr<RP>(B, (const RP*)B->rowptr);
+      run_analysis(h, a, b, s);
+      void* sk = nullptr;
+      OCEAN_CUDA(cudaMallocAsync(&sk, std::max<uint64_t>(B->rows, 1) << log2p, s));
+      launch_hll_sketch_sample(a, b, h->w, log2p, 0u, (uint8_t*)sk, s);
+      launch_hll_rows(a, h->w, log2p, 1.0, 0u, true, (const uint8_t*)sk, est, s);
+      const cudaError_t e = cudaGetLastError();
+      cudaFreeAsync(sk, s);
+      OCEAN_CUDA(e);
+      OCEAN_CUDA(cudaStreamSynchronize(s));
+    };
+    if (A->rowptr_bits == 32) go(uint32_t{});
+    else go(uint64_t{});
   });
 }
 

@@ -58,6 +58,13 @@ struct DevCounters {
   unsigned long long sym_prod[SB_COUNT];  // products of the rows of each symbolic class
   unsigned long long sym_words;           // bitmap words of single-window bitmap-class rows
   unsigned long long cache_cursor;        // words handed out from the bitmap cache
+  unsigned long long total_est;           // estimation workflow: sum of the row-size estimates
+  unsigned int overflow_n;                // estimation workflow: rows that did not fit their estimate
+  unsigned int overflow_cursor[2];        // queue cursors of the overflow recount and rerun
+  unsigned int sample_rows;               // HLL sampling: rows sampled
+  unsigned long long sample_products;     // HLL sampling: products of the sampled rows
+  double sample_est;                      // HLL sampling: raw estimates of the sampled rows
+  double sample_compaction;               // HLL sampling: sum of products / estimate over samples
   unsigned int status;     // OR of DevError bits
   unsigned int err_row;
   unsigned int pad[4];
@@ -67,6 +74,28 @@ enum DevError : unsigned int {
   DEV_TABLE_FULL = 1u,     // an open-addressing probe exceeded the table size
   DEV_BIN_OVERFLOW = 2u,   // a row did not fit the class it was placed in
   DEV_COUNT_MISMATCH = 4u  // numeric output count differs from the symbolic count
+};
+
+constexpr uint32_t kUnknownCount = 0xFFFFFFFFu;
+
+// A device-side list of rows rows[0 .. *count), taken one by one through *cursor.
+struct RowQueue {
+  const uint32_t* rows;
+  const unsigned int* count;
+  unsigned int* cursor;
+};
+
+// Where a numeric kernel writes each row. Exact mode (count == nullptr): row r
+// has exactly cap[r] entries starting at off[r]. Estimation mode: row r has
+// cap[r] slots at off[r]; its true count is stored in count[r] (kUnknownCount
+// when it could not be counted) and a row that does not fit is appended to
+// overflow[] and not written.
+struct OutSpec {
+  const uint64_t* off;
+  const uint32_t* cap;
+  uint32_t* count;
+  uint32_t* overflow;
+  unsigned int* overflow_n;
 };
 
 // CSR view used by kernels. RP is the row-pointer type (uint32_t or uint64_t).

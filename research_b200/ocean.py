@@ -32,7 +32,7 @@ STATUS_NAMES = {0: "OK", 1: "CUDA", 2: "CAPACITY", 3: "TIMEOUT", 4: "INVALID", 5
 EXPORTS = (
     "ocean_create", "ocean_create_from_file", "ocean_destroy", "ocean_spgemm", "ocean_spgemm_host",
     "ocean_csr_free", "ocean_csr_download", "ocean_csr_download_rows", "ocean_symbolic", "ocean_stats_json", "ocean_stage_ms",
-    "ocean_murmur3_u32", "ocean_last_error", "ocean_version", "ocean_symbolic_noalloc",
+    "ocean_murmur3_u32", "ocean_last_error", "ocean_version", "ocean_symbolic_noalloc", "ocean_row_estimates",
 )
 
 
@@ -81,6 +81,7 @@ def lib() -> ctypes.CDLL:
     L.ocean_csr_download_rows.argtypes = [P(CsrOut), u64, u64, vp, vp, vp, vp]
     L.ocean_symbolic.argtypes = [vp, P(CsrView), P(CsrView), vp, vp]
     L.ocean_symbolic_noalloc.argtypes = [P(CsrView), P(CsrView), vp, vp]
+    L.ocean_row_estimates.argtypes = [vp, P(CsrView), P(CsrView), ctypes.c_int, vp, vp]
     L.ocean_stats_json.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, P(ctypes.c_size_t)]
     L.ocean_stage_ms.argtypes = [vp, ctypes.c_char_p]
     L.ocean_stage_ms.restype = ctypes.c_double
@@ -277,6 +278,15 @@ class SpGEMM:
         out = torch.empty(A.rows, dtype=torch.int32, device="cuda")
         av, bv = A.view(), B.view()
         _check(lib().ocean_symbolic(self._h, ctypes.byref(av), ctypes.byref(bv), _ptr(out), stream or None))
+        return out
+
+    def row_estimates(self, A: DeviceCSR, B: Optional[DeviceCSR] = None, log2p: int = 6):
+        """Raw HLL estimate of every row's output count (device tensor, uint32 as int32)."""
+        import torch
+        B = A if B is None else B
+        out = torch.empty(A.rows, dtype=torch.int32, device="cuda")
+        av, bv = A.view(), B.view()
+        _check(lib().ocean_row_estimates(self._h, ctypes.byref(av), ctypes.byref(bv), log2p, _ptr(out), None))
         return out
 
     def get_stats(self) -> dict:

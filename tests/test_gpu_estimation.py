@@ -1,0 +1,92 @@
+"""Estimation workflows on the GPU: HLL row-size estimates against the oracle's
+HLL restatement, and the estimate -> preallocate -> flag overflow -> exact rerun
+protocol (reference: kernels/SpGEMM.cuh:1395-1736) giving the oracle's C."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from research_b200 import matrices as M
+from research_b200.ocean import DeviceCSR, SpGEMM
+
+pytestmark = pytest.mark.gpu
+
+
+def multiply(A, B, cfg):
+    g = SpGEMM(cfg)
+    dA = DeviceCSR.from_host(A)
+    dB = dA if B is A else DeviceCSR.from_host(B)
+    C = g.multiply(dA, dB)
+    h = C.download()
+    C.free()
+    return h, g.get_stats()
+
+
+def check(A, B, C):
+    cp, cj, cx, ca = O.spgemm(A, B, with_abs=True)
+    assert int(C.rowptr[-1]) == C.nnz == int(cp[-1])
+    O.compare(C.rowptr, C.col, C.val, cp, cj, cx, ca, 1e-12)
+
+
+@pytest.mark.parametrize("log2p", [5, 6])
+def test_hll_estimates_match_oracle(log2p):
+    A = M.rmat(13, 16, seed=7)
+    g = SpGEMM()
+    dA = DeviceCSR.from_host(A)
+    got = g.row_estimates(dA, dA, log2p).cpu().numpy().view(np.uint32).astype(np.int64)
+    sk = O.hll_sketch_rows(A, log2p)
+    rp = A.rowptr.astype(np.int64)
+    want = np.array([O.hll_estimate_union(sk, log2p, A.col[rp[i]:rp[i + 1]]) for i in range(A.rows)], np.int64)
+    diff = np.abs(got - want)
+    assert diff.max() <= 1 and (diff == 0).mean() > 0.999
+    # the estimate tracks the exact row size
+    exact = O.symbolic(A, A).astype(np.float64)
+    big = exact >= 256
+    rel = np.abs(got[big] - exact[big]) / exact[big]
+    assert rel.mean() < (0.25 if log2p == 5 else 0.2)
+
+
+@pytest.mark.parametrize("wf", [1, 2])
+@pytest.mark.parametrize("gen", ["uniform", "banded", "rmat14", "rect", "block"])
+def test_estimated_workflows_exact(gen, wf):
+    if gen == "uniform":
+        A = M.uniform_random(20000, 16, seed=1); B = A
+    elif gen == "banded":
+        A = M.banded(30000, 65, 24, seed=2); B = A
+    elif gen == "rmat14":
+        A = M.rmat(14, 16, seed=4); B = A
+    elif gen == "block":
+        A = M.block_diagonal(32768, 256, 32, seed=3); B = A
+    else:
+        A = M.rect_poisson(16384, 65536, 12.0, seed=5); B = M.transpose(A)
+    C, st = multiply(A, B, {"force_workflow": wf, "small_problem_nnz": 0})
+    check(A, B, C)
+    assert st["decision"]["workflow"] == wf and "estimation" in st
+    if wf == 2:
+        assert st["estimation"]["overflow_rows"] == 0  # product counts never underestimate
+
+
+@pytest.mark.parametrize("scale", [0.05, 0.5])
+def test_overflow_rows_are_rerun_exactly(scale):
+    # deliberately low estimates: many rows overflow and go through the exact rerun
+    A = M.rmat(14, 16, seed=9)
+    C, st = multiply(A, A, {"force_workflow": 1, "estimate_scale": scale, "esc_max_products": 0,
+                            "small_problem_nnz": 0})
+    check(A, A, C)
+    assert st["estimation"]["overflow_rows"] > 0
+
+
+def test_automatic_choice():
+    # mean of 48 products per row: ultra-sparse workflow (reference rule: <= 64)
+    A = M.rect_poisson(262144, 1048576, 12.0, seed=0)
+    At = M.transpose(A)
+    C, st = multiply(A, At, {})
+    assert st["decision"]["workflow"] == 2
+    check(A, At, C)
+    # R-MAT: high input expansion, sampled compaction ~2 < 8 -> precise after sampling
+    R = M.rmat(16, 16, seed=0)
+    C, st = multiply(R, R, {"small_problem_nnz": 0})
+    assert st["decision"]["workflow"] == 0 and st["sampling"]["compaction_1"] > 0
+    check(R, R, C)
+    # switched off like the reference's baseline config
+    C, st = multiply(A, At, {"use_estimation_workflow": False, "use_ultrasparse_workflow": False})
+    assert st["decision"]["workflow"] == 0
