@@ -130,6 +130,7 @@ struct ocean_handle {
   uint64_t cap_rows = 0;
   DevCounters* h_ctr = nullptr;  // pinned
   cudaEvent_t ev[EV_COUNT];
+  uint64_t ev_mask = 0;  // events recorded during the last call
   bool ev_recorded = false;
   bool tracked = false;
   Stats st;
@@ -238,7 +239,10 @@ void validate_view(const ocean_csr_view* m, const char* name) {
               std::string(name) + " has nnz >= 2^32 with 32-bit row pointers");
 }
 
-void record(ocean_handle* h, int i, cudaStream_t s) { cudaEventRecord(h->ev[i], s); }
+void record(ocean_handle* h, int i, cudaStream_t s) {
+  cudaEventRecord(h->ev[i], s);
+  h->ev_mask |= 1ull << i;
+}
 
 // Waits for `s` by polling for a short, bounded time before falling back to a
 // blocking synchronize: the mid-call read-backs are tens of microseconds apart
@@ -309,6 +313,8 @@ void make_policies(const Config& c, SymPolicy* sp, NumPolicy* np) {
 // product totals); small inputs skip the read-back. Returns whether it read back.
 template <typename RP>
 bool run_analysis(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s) {
+  h->ev_recorded = false;  // the stats describe a completed multiply only
+  h->ev_mask = 0;
   ensure_rows(h, A.rows);
   OCEAN_CUDA(cudaMemsetAsync(h->w.ctr, 0, sizeof(DevCounters), s));
   SymPolicy sp;
@@ -368,6 +374,7 @@ void run_symbolic(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStrea
   const bool track = h->cfg.track_stage_times;
   h->st.launches += launch_symbolic(A, B, h->w, h->num_sms, s, track ? h->ev + EV_SYM0 : nullptr,
                                     readback ? sym_counts : nullptr);
+  if (track && A.rows) h->ev_mask |= ((1ull << (SB_COUNT + 1)) - 1) << EV_SYM0;
   OCEAN_CUDA(cudaGetLastError());
   if (with_scan) {
     h->st.launches += launch_scan(h->w, h->w.row_nnz, h->w.rowptr64, h->w.rowptr32, &h->w.ctr->total_nnz, true, np, s);
@@ -505,6 +512,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   st.a_rows = A.rows, st.a_cols = A.cols, st.a_nnz = A.nnz;
   st.b_rows = B.rows, st.b_cols = B.cols, st.b_nnz = B.nnz;
   h->ev_recorded = false;
+  h->ev_mask = 0;
   const bool track = h->cfg.track_stage_times;
   NumPolicy np;
   {
@@ -544,6 +552,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         const OutSpec est_out{h->w.est_off, h->w.est, h->w.cnt, h->w.ovf, &h->w.ctr->overflow_n};
         st.launches += launch_numeric(A, B, h->w, est_out, (uint32_t*)t_col, (double*)t_val, h->num_sms, s,
                                       track ? h->ev + EV_NUM0 : nullptr, num_counts);
+        if (track) h->ev_mask |= ((1ull << (NB_COUNT + 1)) - 1) << EV_NUM0;
         // rows that did not fit their estimate: exact counts, then the row pointers
         st.launches += launch_overflow(A, B, h->w, false, nullptr, nullptr, h->num_sms, s);
         st.launches += launch_scan(h->w, h->w.cnt, h->w.rowptr64, h->w.rowptr32, &h->w.ctr->total_nnz, false, np, s);
@@ -571,6 +580,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         const OutSpec exact{h->w.rowptr64, h->w.row_nnz, nullptr, nullptr, nullptr};
         st.launches += launch_numeric(A, B, h->w, exact, owner->col, owner->val, h->num_sms, s,
                                       track ? h->ev + EV_NUM0 : nullptr, num_counts);
+        if (track) h->ev_mask |= ((1ull << (NB_COUNT + 1)) - 1) << EV_NUM0;
       } else {
         launch_copy_rows(h->w, (const uint32_t*)t_col, (const double*)t_val, owner->col, owner->val, s);
         st.launches += 1;
@@ -664,11 +674,15 @@ void dispatch_spgemm(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_v
   run_spgemm<uint64_t>(h, A, B, arp, brp, C, s);
 }
 
+// Milliseconds between two events of the last call; -1 when either was not
+// recorded. A failed query does not leave an error behind for the caller.
 double ev_ms(ocean_handle* h, int a, int b) {
-  if (!h->ev_recorded) return -1.0;
-  if (cudaEventSynchronize(h->ev[b]) != cudaSuccess) return -1.0;
+  if (!h->ev_recorded || !((h->ev_mask >> a) & 1) || !((h->ev_mask >> b) & 1)) return -1.0;
   float ms = 0.f;
-  if (cudaEventElapsedTime(&ms, h->ev[a], h->ev[b]) != cudaSuccess) return -1.0;
+  if (cudaEventSynchronize(h->ev[b]) != cudaSuccess || cudaEventElapsedTime(&ms, h->ev[a], h->ev[b]) != cudaSuccess) {
+    cudaGetLastError();
+    return -1.0;
+  }
   return ms;
 }
 

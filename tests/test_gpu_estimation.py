@@ -90,3 +90,20 @@ def test_automatic_choice():
     # switched off like the reference's baseline config
     C, st = multiply(A, At, {"use_estimation_workflow": False, "use_ultrasparse_workflow": False})
     assert st["decision"]["workflow"] == 0
+
+
+def test_stats_queries_leave_no_cuda_error():
+    # stage timings of stages a workflow did not run are -1, and asking for them
+    # must not leave an error for the next CUDA call of the application
+    import torch
+    A = M.rect_poisson(16384, 65536, 12.0, seed=5)
+    g = SpGEMM({"track_stage_time": True, "force_workflow": 2, "small_problem_nnz": 0})
+    dA = DeviceCSR.from_host(A)
+    dB = DeviceCSR.from_host(M.transpose(A))
+    C = g.multiply(dA, dB)
+    st = g.get_stats()
+    assert st["timing"]["symbolic"] == -1.0 and g.stage_ms("symbolic_esc1") == -1.0
+    C.free()
+    x = torch.ones(1000, device="cuda") * 2  # would raise if an error were pending
+    torch.cuda.synchronize()
+    assert float(x.sum()) == 2000.0
