@@ -121,7 +121,7 @@ int ocean_row_estimates(ocean_handle* h, const ocean_csr_view* A, const ocean_cs
  * caching allocator holds the device memory; or a service forbids cudaMalloc in
  * steady state because it can synchronize the device). No handle: the scratch
  * of the analysis and symbolic kernels is one fixed device array inside the
- * library (about 6.8 MB, held by every GPU that loads the library until exit),
+ * library (about 7.3 MB, held by every GPU that loads the library until exit),
  * so A may have at most 131072 rows (larger A: OCEAN_ERR_INVALID). A and B need
  * the same row-pointer width; row_nnz[A.rows] is the caller's device array. The
  * first call on a device resolves the array's address and must come before any

@@ -1,6 +1,7 @@
 // Host-side launchers of the SpGEMM kernels (implemented in kernels_core.cu).
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 #include "ocean_internal.cuh"
 
@@ -13,6 +14,7 @@ struct DevWork {
   uint32_t* lo = nullptr;        // smallest output column per row (kEmpty if none)
   uint32_t* hi = nullptr;        // largest output column per row
   uint32_t* anz = nullptr;       // entries per row of A
+  uint32_t* maxb = nullptr;      // longest referenced B row per row of A
   uint32_t* row_nnz = nullptr;   // exact output count per row
   uint32_t* sym_bins = nullptr;  // [SB_COUNT][rows] row ids per symbolic class
   uint32_t* num_bins = nullptr;  // [NB_COUNT][rows] row ids per numeric class
@@ -97,5 +99,36 @@ void configure_kernel_attributes();
 
 // Stores the calling thread's error message returned by ocean_last_error().
 void set_last_error(const char* msg);
+
+// ---------------------------------------------------------------- segmentation
+// Spy-plot segmentation of A (reference: kernels/Segmentation.cuh:34-73).
+enum SegClass : uint32_t { SEG_SPARSE_UNIFORM = 0, SEG_DENSE = 1, SEG_POWER_LAW = 2, SEG_BANDED = 3 };
+
+struct SegRecord {
+  uint32_t row_start, row_end, row_count;
+  uint32_t col_left, col_right;  // union of the rows' output column spans
+  uint32_t cls;                  // SegClass
+  unsigned long long sum_products, sum_a_nnz;
+  uint32_t max_b_row_len, max_a_row_len;
+  double mean_row_len;  // mean products per row
+  double var_row_len;   // population variance of products per row
+  double local_er;      // sum_products / sum_a_nnz
+};
+
+struct SegmentationResult {
+  std::vector<SegRecord> segments;
+  uint32_t grid_h = 0, grid_w = 0, tile_rows = 0, tile_cols = 0;
+  uint32_t num_components = 0;
+  double density_mean = 0.0, density_stddev = 0.0;
+  float time_density_ms = 0.f, time_threshold_ms = 0.f, time_cc_ms = 0.f, time_classify_ms = 0.f;
+  int cc_iterations = 0;
+};
+
+// Needs the analysis outputs w.prod, w.anz, w.maxb, w.lo, w.hi of A * B.
+template <typename RP>
+cudaError_t run_segmentation(const Csr<RP>& A, uint64_t b_cols, const DevWork& w, int grid_max, double hot_k,
+                             int min_segment_rows, int cc_max_iters, int expansion_threshold, cudaStream_t s,
+                             SegmentationResult* out);
+const char* segment_class_name(uint32_t cls);
 
 }  // namespace ocean

@@ -128,8 +128,8 @@ __device__ __forceinline__ int num_bin_for(uint32_t n, uint64_t p, uint64_t span
 template <typename RP, int G>
 __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
                                                   uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
-                                                  uint32_t* __restrict__ anz, uint32_t* __restrict__ row_nnz,
-                                                  uint64_t* __restrict__ bm_off,
+                                                  uint32_t* __restrict__ anz, uint32_t* __restrict__ maxb,
+                                                  uint32_t* __restrict__ row_nnz, uint64_t* __restrict__ bm_off,
                                                   uint32_t* __restrict__ sym_bins,
                                                   DevCounters* __restrict__ ctr, SymPolicy pol) {
   __shared__ unsigned long long s_anz[SB_COUNT], s_prod[SB_COUNT], s_words;
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     a1 = A.row_end(row);
   }
   unsigned long long p = 0;
-  uint32_t mn = kEmpty, mx = 0;
+  uint32_t mn = kEmpty, mx = 0, lb = 0;
   for (uint64_t k = a0 + sl; k < a1; k += G) {
     const uint32_t j = A.col[k];
     const uint64_t b0 = B.row_begin(j), b1 = B.row_end(j);
@@ -157,6 +157,7 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
       p += b1 - b0;
       mn = min(mn, B.col[b0]);
       mx = max(mx, B.col[b1 - 1]);
+      lb = max(lb, (uint32_t)min(b1 - b0, (uint64_t)0xFFFFFFFFu));
     }
   }
 #pragma unroll
@@ -164,6 +165,7 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     p += __shfl_xor_sync(kFull, p, o);
     mn = min(mn, __shfl_xor_sync(kFull, mn, o));
     mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+    lb = max(lb, __shfl_xor_sync(kFull, lb, o));
   }
   int b = -1;
   const bool leader = valid && sl == 0;
@@ -172,6 +174,7 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     lo[row] = mn;
     hi[row] = mx;
     anz[row] = (uint32_t)(a1 - a0);
+    maxb[row] = lb;
     bm_off[row] = ~0ull;
     if (p == 0) {
       row_nnz[row] = 0;
@@ -1371,11 +1374,11 @@ int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const 
   if (avg >= 12.0) {
     const uint64_t threads = A.rows * 32;
     k_analysis<RP, 32><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
+        A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
   } else {
     const uint64_t threads = A.rows * 4;
     k_analysis<RP, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.anz, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
+        A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
   }
   return 1;
 }

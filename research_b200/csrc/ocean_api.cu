@@ -134,6 +134,9 @@ struct ocean_handle {
   bool ev_recorded = false;
   bool tracked = false;
   Stats st;
+  // spy-plot segmentation of the last multiply (use_segmented_workflow)
+  SegmentationResult seg;
+  bool seg_ran = false;
   // widened row pointers for mixed 32/64-bit inputs
   uint64_t* wide_a = nullptr;
   uint64_t wide_a_cap = 0;
@@ -160,7 +163,7 @@ struct ocean_handle {
 
   void free_all() {
     DevWork& x = w;
-    void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
+    void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.maxb, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
                   x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf, x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
     for (void* p : ps)
       if (p) cudaFree(p);
@@ -202,13 +205,14 @@ void ensure_rows(ocean_handle* h, uint64_t rows) {
     return;
   }
   DevWork& x = h->w;
-  void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64, x.rowptr32,
-                x.bm_off, x.est, x.est_off, x.cnt, x.ovf};
+  void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.maxb, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
+                x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf};
   for (void* p : ps)
     if (p) cudaFree(p);
   const uint64_t r = std::max<uint64_t>(rows, 1);
   OCEAN_CUDA(cudaMalloc((void**)&x.prod, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.anz, r * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&x.maxb, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.lo, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.hi, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.row_nnz, r * 4));
@@ -513,6 +517,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   st.b_rows = B.rows, st.b_cols = B.cols, st.b_nnz = B.nnz;
   h->ev_recorded = false;
   h->ev_mask = 0;
+  h->seg_ran = false;
   const bool track = h->cfg.track_stage_times;
   NumPolicy np;
   {
@@ -528,6 +533,14 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   try {
     if (A.rows > 0) {
       const bool readback = run_analysis(h, A, B, s);
+      if (h->cfg.use_segmented_workflow) {
+        // analysis-only pass: its records go to the stats (reference: kernels/SpGEMM.cuh:240-259)
+        const Config& c = h->cfg;
+        OCEAN_CUDA(run_segmentation(A, B.cols, h->w, c.segmentation_grid_max, c.segmentation_hot_threshold_k,
+                                    c.segmentation_min_segment_rows, c.segmentation_cc_max_iters,
+                                    c.estimation_input_expansion_threshold, s, &h->seg));
+        h->seg_ran = true;
+      }
       wf = choose_workflow(h, A, B, s, readback);
       if (wf == WF_ESTIMATION || wf == WF_ULTRASPARSE) {
         // scan of the estimates: temporary slots per row, numeric classes by estimate
@@ -714,6 +727,28 @@ std::string stats_json(ocean_handle* h) {
   if (st.workflow == 1 || st.workflow == 2)
     o << "\"estimation\": {\"overflow_rows\": " << st.overflow_rows << ", \"log2_precision\": " << st.hll_log2p
       << ", \"total_est\": " << st.total_est << ", \"expansion\": " << st.hll_expansion << "}, ";
+  if (h->seg_ran) {
+    // reference: kernels/SpGEMM.cuh:1851-1886
+    const SegmentationResult& g = h->seg;
+    o << "\"segmentation\": {\"grid_h\": " << g.grid_h << ", \"grid_w\": " << g.grid_w
+      << ", \"tile_rows\": " << g.tile_rows << ", \"tile_cols\": " << g.tile_cols
+      << ", \"density_mean\": " << g.density_mean << ", \"density_stddev\": " << g.density_stddev
+      << ", \"num_components\": " << g.num_components << ", \"cc_iterations\": " << g.cc_iterations
+      << ", \"time_density_ms\": " << g.time_density_ms << ", \"time_threshold_ms\": " << g.time_threshold_ms
+      << ", \"time_cc_ms\": " << g.time_cc_ms << ", \"time_classify_ms\": " << g.time_classify_ms
+      << ", \"segments\": [";
+    for (size_t i = 0; i < g.segments.size(); ++i) {
+      const SegRecord& r = g.segments[i];
+      o << (i ? ", " : "") << "{\"row_start\": " << r.row_start << ", \"row_end\": " << r.row_end
+        << ", \"row_count\": " << r.row_count << ", \"col_left\": " << r.col_left
+        << ", \"col_right\": " << r.col_right << ", \"class\": \"" << segment_class_name(r.cls)
+        << "\", \"sum_products\": " << r.sum_products << ", \"sum_a_nnz\": " << r.sum_a_nnz
+        << ", \"mean_row_len\": " << r.mean_row_len << ", \"var_row_len\": " << r.var_row_len
+        << ", \"local_er\": " << r.local_er << ", \"max_b_row_len\": " << r.max_b_row_len
+        << ", \"max_a_row_len\": " << r.max_a_row_len << "}";
+    }
+    o << "]}, ";
+  }
   o << "\"binning_1\": [";
   for (int i = 0; i < SB_COUNT; ++i) o << (i ? ", " : "") << st.sym_bins[i];
   o << "], \"binning_2\": [";

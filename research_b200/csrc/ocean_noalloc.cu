@@ -11,7 +11,7 @@
 //
 // How: all scratch of the analysis and symbolic kernels (per-row products,
 // column spans, A-row lengths, class lists and the device counters) lives in
-// one file-scope device array of fixed size, kNoAllocScratchBytes (about 6.8 MB),
+// one file-scope device array of fixed size, kNoAllocScratchBytes (about 7.3 MB),
 // which every GPU that loads this library holds until the process exits. It
 // bounds A to kNoAllocMaxRows rows; larger inputs are rejected with
 // OCEAN_ERR_INVALID before any work. Inputs and the output array row_nnz are
@@ -39,7 +39,7 @@ namespace {
 constexpr uint64_t kNoAllocMaxRows = 131072;
 constexpr uint64_t kCountersBytes = 1024;
 constexpr uint64_t kNoAllocScratchBytes =
-    kCountersBytes + kNoAllocMaxRows * (4 /*prod*/ + 4 /*lo*/ + 4 /*hi*/ + 4 /*anz*/ + 8 /*bm_off*/ +
+    kCountersBytes + kNoAllocMaxRows * (4 /*prod*/ + 4 /*lo*/ + 4 /*hi*/ + 4 /*anz*/ + 4 /*maxb*/ + 8 /*bm_off*/ +
                                         4 * (uint64_t)SB_COUNT /*class lists*/);
 static_assert(sizeof(DevCounters) <= kCountersBytes, "counters do not fit their slot");
 
@@ -95,6 +95,8 @@ int run_noalloc(const ocean_csr_view* A, const ocean_csr_view* B, uint32_t* row_
   w.hi = reinterpret_cast<uint32_t*>(p);
   p += R * 4;
   w.anz = reinterpret_cast<uint32_t*>(p);
+  p += R * 4;
+  w.maxb = reinterpret_cast<uint32_t*>(p);
   p += R * 4;
   w.sym_bins = reinterpret_cast<uint32_t*>(p);  // class lists are strided by A->rows (<= R)
   w.row_nnz = row_nnz;
