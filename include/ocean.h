@@ -131,6 +131,63 @@ int ocean_row_estimates(ocean_handle* h, const ocean_csr_view* A, const ocean_cs
 int ocean_symbolic_noalloc(const ocean_csr_view* A, const ocean_csr_view* B, uint32_t* row_nnz,
                            void* stream);
 
+/* ---- Learned row-size estimator -------------------------------------------
+ * A 3-layer perceptron (16 features -> 64 -> 64 -> 1, ReLU) predicting
+ * t = log2(1 + nnz of an output row). Its GEMMs run on the tensor cores with
+ * BF16 weights/activations and FP32 accumulation. With the config key
+ * "use_learned_estimator" it replaces the HLL estimate that sizes each row in
+ * the estimation workflow (the reference's estimator: kernels/HLL.cuh:107-236
+ * feeding kernels/SpGEMM.cuh:1395-1480); rows that outgrow the estimate are
+ * counted and recomputed exactly, so C is unchanged. No counterpart in the
+ * reference. The entry points below train and check the network; all pointers
+ * except `blob` are device pointers. */
+#define OCEAN_MLP_FEATURES 16
+#define OCEAN_MLP_PARAMS 5313 /* W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3 */
+#define OCEAN_MLP_BLOB 5346   /* params, mu[16], inv_sd[16], margin */
+
+typedef struct {
+  const float* params; /* OCEAN_MLP_PARAMS floats; weights are rounded to BF16 on use */
+  const float* mu;     /* feature means (16) */
+  const float* inv_sd; /* inverse feature standard deviations (16) */
+  float margin;        /* log2 margin added before an estimate sizes a row */
+} ocean_mlp_model;
+
+/* Raw features of every row of A·B into feat[A.rows][16] (row analysis plus
+ * the raw 32-register HLL union estimate). Waits for the result. */
+int ocean_mlp_features(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, float* feat,
+                       void* stream);
+/* pred[i] = network output for feat[i] (i < n). Waits for the result. */
+int ocean_mlp_forward(ocean_handle* h, const ocean_mlp_model* m, const float* feat, uint64_t n, float* pred,
+                      void* stream);
+/* Forward and backward pass of L = sum_i (pred_i - target_i)^2 / batch over
+ * the n rows: dL/dparams is ADDED to grad[OCEAN_MLP_PARAMS] and the sum of
+ * squared errors to *loss. Waits for the result. */
+int ocean_mlp_grad(ocean_handle* h, const ocean_mlp_model* m, const float* feat, const float* target, uint64_t n,
+                   float batch, float* grad, float* loss, void* stream);
+/* One Adam step (bias-corrected, step >= 1) on params; zeroes grad. */
+int ocean_mlp_adam(ocean_handle* h, float* params, float* m1, float* m2, float* grad, int step, float lr,
+                   float beta1, float beta2, float eps, void* stream);
+/* Copies the built-in trained network (OCEAN_MLP_BLOB floats) to host `blob`. */
+int ocean_mlp_builtin(float* blob, size_t n);
+
+/* Per-row output-size estimates of A·B into est[A.rows], made as the
+ * estimation workflow makes them. estimator 1 = HLL (kernels/HLL.cuh:107-236:
+ * log2 precision 5 or 6 by the reference's rule; with_margin: times the
+ * expansion 2.0 / 1.5, else the union estimate itself; clamped to
+ * [1, min(products, span)]); 2 = the learned network (with_margin: plus its
+ * log2 margin; clamped to [max(1, longest B row), min(products, span)]).
+ * Rows of at most esc_max_products products get their product count. */
+int ocean_estimate(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, int estimator,
+                   int with_margin, uint32_t* est, void* stream);
+/* Quality of est[] against exact counts truth[] (device arrays) for the rows
+ * of the handle's last analysed A·B (ocean_estimate or ocean_symbolic with
+ * the same A and B) that have more than min_products products (0: all rows
+ * with output): out[0] mean |est - truth| / truth; out[1] percent of them
+ * whose numeric class differs; out[2] their number; out[3] rows with
+ * est < truth (they would be rerun). */
+int ocean_estimate_metrics(ocean_handle* h, const uint32_t* est, const uint32_t* truth, uint32_t min_products,
+                           double* out, void* stream);
+
 /* Stats of the last multiply as JSON text, with the reference's keys
  * (kernels/SpGEMM.cuh:1788-1890: "A","B","C","stats","decision","timing",
  * "total_time","gflops", ...). If cap is too small, *needed gets the size. */

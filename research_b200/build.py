@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
 
-LIB_SOURCES = ["kernels_core.cu", "segmentation.cu", "ocean_api.cu", "ocean_noalloc.cu"]
+LIB_SOURCES = ["kernels_core.cu", "segmentation.cu", "mlp.cu", "ocean_api.cu", "ocean_noalloc.cu"]
 HEADERS = ["ocean_internal.cuh", "kernels.h", "config.h"]
 
 

@@ -191,6 +191,10 @@ struct Config {
   int spin_wait_us = 2000;              // poll the stream this long before a blocking synchronize
   int force_workflow = -1;              // -1 auto; 0 precise, 1 estimation (HLL), 2 ultra-sparse
   double estimate_scale = 1.0;          // multiplies the HLL expansion (testing: < 1 forces overflows)
+  bool use_learned_estimator = false;   // estimation workflow: per-row sizes from the MLP instead of HLL
+  std::string learned_estimator_weights;  // weights file; empty: the built-in trained network
+  double learned_margin_scale = 1.0;    // multiplies the network's log2 preallocation margin
+  bool estimator_metrics = false;       // after an estimated multiply: error of the estimates vs exact counts
 
   static Config from_json_text(const std::string& text) {
     Config c;
@@ -256,6 +260,10 @@ struct Config {
     geti("spin_wait_us", c.spin_wait_us);
     geti("force_workflow", c.force_workflow);
     getd("estimate_scale", c.estimate_scale);
+    getb("use_learned_estimator", c.use_learned_estimator);
+    gets("learned_estimator_weights", c.learned_estimator_weights);
+    getd("learned_margin_scale", c.learned_margin_scale);
+    getb("estimator_metrics", c.estimator_metrics);
     if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
     if (c.force_workflow < -1 || c.force_workflow > 2)

@@ -97,29 +97,6 @@ __device__ __forceinline__ bool out_accept(const OutSpec& o, DevCounters* ctr, u
   return false;
 }
 
-// Symbolic class of a row from its product count and output column span.
-__device__ __forceinline__ int sym_bin_for(uint64_t p, uint64_t span, const SymPolicy& pol) {
-  if (pol.force_bin >= 0) return pol.force_bin;
-  if (p <= pol.esc_max_products) return p <= 32 ? SB_ESC1 : (p <= 64 ? SB_ESC2 : SB_ESC4);
-  const uint64_t words = (span + 63) >> 6;
-  if (p > 16384) return SB_BITMAP;
-  if (p <= 1024) return SB_HASH_S;
-  if (p <= 4096) return (words <= 2048) ? SB_BITMAP : SB_HASH_M;
-  return (words <= 8192) ? SB_BITMAP : SB_HASH_L;
-}
-
-// Numeric class of a row from its exact output count.
-__device__ __forceinline__ int num_bin_for(uint32_t n, uint64_t p, uint64_t span,
-                                           const NumPolicy& pol) {
-  if (n == 0) return -1;
-  if (pol.force_bin >= 0) return pol.force_bin;
-  if (p <= pol.esc_max_products) return p <= 32 ? NB_ESC1 : (p <= 64 ? NB_ESC2 : NB_ESC4);
-  const uint64_t words = (span + 63) >> 6;
-  if (n <= 512) return NB_HASH_S;
-  if (n <= 2048) return (words <= 1024) ? NB_BITMAP : NB_HASH_M;
-  if (n <= 4096) return (words <= 4096) ? NB_BITMAP : NB_HASH_L;
-  return NB_BITMAP;
-}
 
 // ---------------------------------------------------------------- analysis
 // One group of G lanes per row of A: products, output column span; then the

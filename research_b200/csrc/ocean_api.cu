@@ -18,7 +18,10 @@
 
 #include "config.h"
 #include "kernels.h"
+#include "mlp.h"
 #include "ocean.h"
+
+#include "mlp_weights.inc"
 
 using namespace ocean;
 
@@ -91,6 +94,13 @@ struct Stats {
   int rowptr_bits = 32;
   bool valid = false;
   double host_ms = 0.0;
+  // estimation workflows: which estimator sized the rows, and (estimator_metrics)
+  // its error against the exact counts: mean relative row-size error and share
+  // of rows whose numeric class differs, with and without the safety margin
+  int estimator = 0;  // 0 none, 1 HLL, 2 learned
+  bool metrics = false;
+  double mre = 0.0, misbinned = 0.0, mre_raw = 0.0, misbinned_raw = 0.0;
+  uint64_t metric_rows = 0;
 };
 
 __global__ void k_widen_rowptr(const uint32_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t n) {
@@ -134,6 +144,13 @@ struct ocean_handle {
   bool ev_recorded = false;
   bool tracked = false;
   Stats st;
+  // learned estimator: device blob (parameters | mu | inv_sd), margin
+  float* mlp_dev = nullptr;
+  float mlp_margin = 0.f;
+  bool mlp_ready = false;
+  uint32_t* raw_est = nullptr;  // estimator_metrics: estimates without the margin
+  uint64_t raw_est_cap = 0;
+  double* metrics_dev = nullptr;  // 2 x 4 sums of launch_est_metrics
   // spy-plot segmentation of the last multiply (use_segmented_workflow)
   SegmentationResult seg;
   bool seg_ran = false;
@@ -172,6 +189,9 @@ struct ocean_handle {
     if (out_col) cudaFreeHost(out_col);
     if (out_val) cudaFreeHost(out_val);
     if (cache_buf) cudaFree(cache_buf);
+    if (mlp_dev) cudaFree(mlp_dev);
+    if (raw_est) cudaFree(raw_est);
+    if (metrics_dev) cudaFree(metrics_dev);
     for (auto& e : ev) cudaEventDestroy(e);
   }
 };
@@ -191,6 +211,7 @@ void init_handle(ocean_handle* h, const std::string& json) {
   static bool configured[64] = {false};
   if (h->device < 64 && !configured[h->device]) {
     configure_kernel_attributes();
+    configure_mlp_attributes();
     OCEAN_CUDA(cudaGetLastError());
     configured[h->device] = true;
   }
@@ -265,6 +286,7 @@ const char* status_text(unsigned st) {
   if (st & DEV_TABLE_FULL) return "a shared-memory hash table ran full (probe limit reached)";
   if (st & DEV_BIN_OVERFLOW) return "a row exceeded the capacity of its accumulator class";
   if (st & DEV_COUNT_MISMATCH) return "numeric output count differs from the symbolic count";
+  if (st & DEV_TC_TIMEOUT) return "a tensor-core completion wait timed out";
   return "device error";
 }
 
@@ -273,7 +295,9 @@ void check_device_status(ocean_handle* h) {
     char buf[256];
     snprintf(buf, sizeof buf, "%s (status 0x%x, first row %u)", status_text(h->h_ctr->status), h->h_ctr->status,
              h->h_ctr->err_row);
-    throw OceanError{(h->h_ctr->status & DEV_COUNT_MISMATCH) ? (int)OCEAN_ERR_INTERNAL : (int)OCEAN_ERR_CAPACITY,
+    const unsigned st = h->h_ctr->status;
+    throw OceanError{(st & DEV_COUNT_MISMATCH) ? (int)OCEAN_ERR_INTERNAL
+                                               : (st & DEV_TC_TIMEOUT) ? (int)OCEAN_ERR_TIMEOUT : (int)OCEAN_ERR_CAPACITY,
                      buf};
   }
 }
@@ -415,6 +439,59 @@ void drop_cache_buffer(ocean_handle* h, cudaStream_t s) {
   h->cache_cap_words = 0;
 }
 
+// Loads the estimator network once: from learned_estimator_weights (text:
+// the tag "ocean-mlp-v1", then kMlpBlob numbers) or the built-in one.
+void load_model(ocean_handle* h) {
+  if (h->mlp_ready) return;
+  std::vector<float> blob(kMlpBlob);
+  const std::string& path = h->cfg.learned_estimator_weights;
+  if (!path.empty()) {
+    std::ifstream f(path);
+    OCEAN_CHECK(f.good(), OCEAN_ERR_INVALID, "cannot open learned_estimator_weights file");
+    std::string tag;
+    f >> tag;
+    OCEAN_CHECK(tag == "ocean-mlp-v1", OCEAN_ERR_INVALID, "learned_estimator_weights: not an ocean-mlp-v1 file");
+    for (auto& x : blob) f >> x;
+    OCEAN_CHECK(!f.fail(), OCEAN_ERR_INVALID, "learned_estimator_weights: expected 5346 numbers");
+  } else {
+    OCEAN_CHECK(kMlpBuiltinTrained != 0, OCEAN_ERR_INVALID,
+                "no trained estimator is built in; set learned_estimator_weights");
+    std::copy(kMlpBuiltin, kMlpBuiltin + kMlpBlob, blob.begin());
+  }
+  if (!h->mlp_dev) OCEAN_CUDA(cudaMalloc((void**)&h->mlp_dev, kMlpBlob * sizeof(float)));
+  OCEAN_CUDA(cudaMemcpy(h->mlp_dev, blob.data(), kMlpBlob * sizeof(float), cudaMemcpyHostToDevice));
+  h->mlp_margin = blob[kMlpBlob - 1];
+  h->mlp_ready = true;
+}
+
+MlpModel model_of(const ocean_handle* h) {
+  MlpModel m;
+  m.params = h->mlp_dev;
+  m.mu = h->mlp_dev + kMlpParams;
+  m.inv_sd = m.mu + kMlpF;
+  m.margin = h->mlp_margin * (float)h->cfg.learned_margin_scale;
+  return m;
+}
+
+// The estimator's per-row inputs: the analysis arrays, the raw HLL estimates
+// in w.est, and two scalars of B.
+template <typename RP>
+MlpRowInputs row_inputs(const ocean_handle* h, const Csr<RP>& B) {
+  MlpRowInputs in;
+  in.anz = h->w.anz;
+  in.prod = h->w.prod;
+  in.lo = h->w.lo;
+  in.hi = h->w.hi;
+  in.maxb = h->w.maxb;
+  in.hll = h->w.est;
+  in.log_b_cols = log2f(1.f + (float)B.cols);
+  in.log_b_avg = log2f(1.f + (B.rows ? (float)((double)B.nnz / (double)B.rows) : 0.f));
+  return in;
+}
+
+// Log2 precision of the HLL sketch the learned estimator's features use.
+constexpr int kLearnedLog2p = 5;
+
 // Workflow ids as reported in the stats (reference: kernels/SpGEMM.cuh:1807-1817).
 enum Workflow { WF_PRECISE = 0, WF_ESTIMATION = 1, WF_ULTRASPARSE = 2 };
 
@@ -447,7 +524,10 @@ int choose_workflow(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStr
   }
   // HLL estimates and sampled compaction
   const uint64_t ratio = A.nnz ? products / A.nnz : 0;
-  const int log2p = (readback && ratio >= (uint64_t)c.hll_higher_precision_expansion_threshold) ? 6 : 5;
+  const bool learned = c.use_learned_estimator;
+  if (learned) load_model(h);
+  const int log2p = learned ? kLearnedLog2p
+                            : (readback && ratio >= (uint64_t)c.hll_higher_precision_expansion_threshold) ? 6 : 5;
   const double expansion = (log2p == 5 ? 2.0 : 1.5) * c.estimate_scale;
   int samples = (int)(A.rows * c.hll_sample_rate);
   samples = std::max(samples, c.hll_sample_min_rows);
@@ -470,8 +550,24 @@ int choose_workflow(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStr
                                               h->st.compaction2 < c.estimation_output_compaction_threshold))
       wf = WF_PRECISE;
     if (wf == WF_ESTIMATION) {
-      h->st.launches += launch_hll_rows(A, h->w, log2p, expansion, (uint32_t)c.esc_max_products, false,
-                                        (const uint8_t*)sk, h->w.est, s);
+      uint32_t* raw = nullptr;
+      if (c.estimator_metrics) {
+        grow(h->raw_est, h->raw_est_cap, A.rows);
+        raw = h->raw_est;
+      }
+      if (learned) {
+        // raw HLL estimates become a feature; the network then writes the estimates over them
+        h->st.launches += launch_hll_rows(A, h->w, log2p, 1.0, 0u, true, (const uint8_t*)sk, h->w.est, s);
+        h->st.launches += launch_mlp_estimate(model_of(h), row_inputs(h, B), A.rows, (uint32_t)c.esc_max_products,
+                                              h->w.est, raw, &h->w.ctr->status, h->num_sms, s);
+        h->st.estimator = 2;
+      } else {
+        if (raw) h->st.launches += launch_hll_rows(A, h->w, log2p, 1.0, (uint32_t)c.esc_max_products, false,
+                                                   (const uint8_t*)sk, raw, s);
+        h->st.launches += launch_hll_rows(A, h->w, log2p, expansion, (uint32_t)c.esc_max_products, false,
+                                          (const uint8_t*)sk, h->w.est, s);
+        h->st.estimator = 1;
+      }
       OCEAN_CUDA(cudaGetLastError());
     }
   } catch (...) {
@@ -480,6 +576,28 @@ int choose_workflow(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStr
   }
   cudaFreeAsync(sk, s);
   return wf;
+}
+
+// estimator_metrics: error of the preallocated estimates (w.est) and of the
+// estimates without margin/expansion (raw_est) against the exact counts (w.cnt).
+template <typename RP>
+void measure_estimates(ocean_handle* h, const Csr<RP>& B, const NumPolicy& np, cudaStream_t s) {
+  if (!h->metrics_dev) OCEAN_CUDA(cudaMalloc((void**)&h->metrics_dev, 8 * sizeof(double)));
+  OCEAN_CUDA(cudaMemsetAsync(h->metrics_dev, 0, 8 * sizeof(double), s));
+  const MlpRowInputs in = row_inputs(h, B);
+  launch_est_metrics(h->w.est, h->w.cnt, in, h->w.rows, np, 0u, h->metrics_dev, s);
+  launch_est_metrics(h->raw_est, h->w.cnt, in, h->w.rows, np, 0u, h->metrics_dev + 4, s);
+  h->st.launches += 2;
+  double m[8];
+  OCEAN_CUDA(cudaMemcpyAsync(m, h->metrics_dev, sizeof m, cudaMemcpyDeviceToHost, s));
+  OCEAN_CUDA(cudaStreamSynchronize(s));
+  Stats& st = h->st;
+  st.metrics = true;
+  st.metric_rows = (uint64_t)m[1];
+  st.mre = m[1] > 0 ? m[0] / m[1] : 0.0;
+  st.mre_raw = m[5] > 0 ? m[4] / m[5] : 0.0;
+  st.misbinned = m[1] > 0 ? 100.0 * m[2] / m[1] : 0.0;
+  st.misbinned_raw = m[5] > 0 ? 100.0 * m[6] / m[5] : 0.0;
 }
 
 // C's buffers; if they do not fit and bitmaps are saved, the bitmaps are
@@ -575,6 +693,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         check_device_status(h);
         nnz = h->h_ctr->total_nnz;
         st.overflow_rows = h->h_ctr->overflow_n;
+        if (h->cfg.estimator_metrics && st.estimator != 0) measure_estimates(h, B, np, s);
       }
     } else {
       std::memset(h->h_ctr, 0, sizeof(DevCounters));
@@ -724,9 +843,16 @@ std::string stats_json(ocean_handle* h) {
   if (st.sampled)
     o << "\"sampling\": {\"compaction_1\": " << st.compaction1 << ", \"compaction_2\": " << st.compaction2
       << "}, ";
-  if (st.workflow == 1 || st.workflow == 2)
+  if (st.workflow == 1 || st.workflow == 2) {
     o << "\"estimation\": {\"overflow_rows\": " << st.overflow_rows << ", \"log2_precision\": " << st.hll_log2p
-      << ", \"total_est\": " << st.total_est << ", \"expansion\": " << st.hll_expansion << "}, ";
+      << ", \"total_est\": " << st.total_est << ", \"expansion\": " << st.hll_expansion << ", \"estimator\": \""
+      << (st.estimator == 2 ? "learned" : st.estimator == 1 ? "hll" : "products") << "\"";
+    if (st.metrics)
+      o << ", \"metrics\": {\"rows\": " << st.metric_rows << ", \"mean_rel_error\": " << st.mre
+        << ", \"misbinned_pct\": " << st.misbinned << ", \"mean_rel_error_raw\": " << st.mre_raw
+        << ", \"misbinned_pct_raw\": " << st.misbinned_raw << "}";
+    o << "}, ";
+  }
   if (h->seg_ran) {
     // reference: kernels/SpGEMM.cuh:1851-1886
     const SegmentationResult& g = h->seg;
@@ -804,6 +930,30 @@ int guarded(F&& f) {
 namespace ocean {
 void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 }  // namespace ocean
+
+namespace {
+MlpModel model_from(const ocean_mlp_model* m) {
+  OCEAN_CHECK(m != nullptr && m->params && m->mu && m->inv_sd, OCEAN_ERR_INVALID, "model pointers are NULL");
+  MlpModel x;
+  x.params = m->params;
+  x.mu = m->mu;
+  x.inv_sd = m->inv_sd;
+  x.margin = m->margin;
+  return x;
+}
+
+// Runs one MLP launch with the handle's status word and reports a timeout.
+template <typename F>
+void with_status(ocean_handle* h, cudaStream_t s, F&& launch) {
+  OCEAN_CUDA(cudaMemsetAsync(&h->w.ctr->status, 0, sizeof(unsigned), s));
+  launch(&h->w.ctr->status);
+  OCEAN_CUDA(cudaGetLastError());
+  OCEAN_CUDA(cudaMemcpyAsync(&h->h_ctr->status, &h->w.ctr->status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  OCEAN_CUDA(cudaStreamSynchronize(s));
+  h->h_ctr->err_row = 0;
+  check_device_status(h);
+}
+}  // namespace
 
 extern "C" {
 
@@ -1022,6 +1172,163 @@ int ocean_row_estimates(ocean_handle* h, const ocean_csr_view* A, const ocean_cs
     };
     if (A->rowptr_bits == 32) go(uint32_t{});
     else go(uint64_t{});
+  });
+}
+
+int ocean_mlp_features(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, float* feat,
+                       void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    validate_view(A, "A");
+    validate_view(B, "B");
+    OCEAN_CHECK(A->cols == B->rows, OCEAN_ERR_INVALID, "Incompatible matrix dimensions (A.cols != B.rows)");
+    OCEAN_CHECK(A->rowptr_bits == B->rowptr_bits, OCEAN_ERR_INVALID,
+                "ocean_mlp_features needs equal row-pointer widths for A and B");
+    OCEAN_CHECK(A->rows == 0 || feat != nullptr, OCEAN_ERR_INVALID, "feat is NULL");
+    if (A->rows == 0) return;
+    cudaStream_t s = (cudaStream_t)stream;
+    auto go = [&](auto rp_tag) {
+      using RP = decltype(rp_tag);
+      const Csr<RP> a = to_csr<RP>(A, (const RP*)A->rowptr), b = to_csr<RP>(B, (const RP*)B->rowptr);
+      run_analysis(h, a, b, s);
+      void* sk = nullptr;
+      OCEAN_CUDA(cudaMallocAsync(&sk, std::max<uint64_t>(B->rows, 1) << kLearnedLog2p, s));
+      launch_hll_sketch_sample(a, b, h->w, kLearnedLog2p, 0u, (uint8_t*)sk, s);
+      launch_hll_rows(a, h->w, kLearnedLog2p, 1.0, 0u, true, (const uint8_t*)sk, h->w.est, s);
+      launch_mlp_features(row_inputs(h, b), a.rows, feat, s);
+      const cudaError_t e = cudaGetLastError();
+      cudaFreeAsync(sk, s);
+      OCEAN_CUDA(e);
+      OCEAN_CUDA(cudaStreamSynchronize(s));
+    };
+    if (A->rowptr_bits == 32) go(uint32_t{});
+    else go(uint64_t{});
+  });
+}
+
+
+int ocean_mlp_forward(ocean_handle* h, const ocean_mlp_model* m, const float* feat, uint64_t n, float* pred,
+                      void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    const MlpModel mm = model_from(m);
+    OCEAN_CHECK(n == 0 || (feat && pred), OCEAN_ERR_INVALID, "feat or pred is NULL");
+    OCEAN_CHECK(((uintptr_t)feat & 15) == 0, OCEAN_ERR_INVALID, "feat must be 16-byte aligned");
+    if (n == 0) return;
+    cudaStream_t s = (cudaStream_t)stream;
+    with_status(h, s, [&](unsigned* st) { launch_mlp_forward(mm, feat, n, pred, st, h->num_sms, s); });
+  });
+}
+
+int ocean_mlp_grad(ocean_handle* h, const ocean_mlp_model* m, const float* feat, const float* target, uint64_t n,
+                   float batch, float* grad, float* loss, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    const MlpModel mm = model_from(m);
+    OCEAN_CHECK(n == 0 || (feat && target && grad && loss), OCEAN_ERR_INVALID, "an array pointer is NULL");
+    OCEAN_CHECK(((uintptr_t)feat & 15) == 0, OCEAN_ERR_INVALID, "feat must be 16-byte aligned");
+    OCEAN_CHECK(batch > 0.f, OCEAN_ERR_INVALID, "batch must be positive");
+    if (n == 0) return;
+    cudaStream_t s = (cudaStream_t)stream;
+    with_status(h, s,
+                [&](unsigned* st) { launch_mlp_grad(mm, feat, target, n, batch, grad, loss, st, h->num_sms, s); });
+  });
+}
+
+int ocean_mlp_adam(ocean_handle* h, float* params, float* m1, float* m2, float* grad, int step, float lr,
+                   float beta1, float beta2, float eps, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    OCEAN_CHECK(params && m1 && m2 && grad, OCEAN_ERR_INVALID, "an array pointer is NULL");
+    OCEAN_CHECK(step >= 1, OCEAN_ERR_INVALID, "step must be >= 1");
+    launch_mlp_adam(params, m1, m2, grad, step, lr, beta1, beta2, eps, (cudaStream_t)stream);
+    OCEAN_CUDA(cudaGetLastError());
+  });
+}
+
+int ocean_mlp_builtin(float* blob, size_t n) {
+  return guarded([&] {
+    OCEAN_CHECK(kMlpBuiltinTrained != 0, OCEAN_ERR_INVALID, "no trained estimator is built in");
+    OCEAN_CHECK(blob != nullptr && n >= (size_t)kMlpBlob, OCEAN_ERR_INVALID, "blob too small");
+    std::memcpy(blob, kMlpBuiltin, kMlpBlob * sizeof(float));
+  });
+}
+
+int ocean_estimate(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_view* B, int estimator,
+                   int with_margin, uint32_t* est, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    validate_view(A, "A");
+    validate_view(B, "B");
+    OCEAN_CHECK(A->cols == B->rows, OCEAN_ERR_INVALID, "Incompatible matrix dimensions (A.cols != B.rows)");
+    OCEAN_CHECK(A->rowptr_bits == B->rowptr_bits, OCEAN_ERR_INVALID,
+                "ocean_estimate needs equal row-pointer widths for A and B");
+    OCEAN_CHECK(estimator == 1 || estimator == 2, OCEAN_ERR_INVALID, "estimator must be 1 (HLL) or 2 (learned)");
+    OCEAN_CHECK(A->rows == 0 || est != nullptr, OCEAN_ERR_INVALID, "est is NULL");
+    if (A->rows == 0) return;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Config& c = h->cfg;
+    auto go = [&](auto rp_tag) {
+      using RP = decltype(rp_tag);
+      const Csr<RP> a = to_csr<RP>(A, (const RP*)A->rowptr), b = to_csr<RP>(B, (const RP*)B->rowptr);
+      run_analysis(h, a, b, s);
+      OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+      OCEAN_CUDA(cudaStreamSynchronize(s));
+      const uint64_t ratio = a.nnz ? h->h_ctr->total_products / a.nnz : 0;
+      const bool learned = estimator == 2;
+      if (learned) load_model(h);
+      const int log2p = learned ? kLearnedLog2p
+                                : (ratio >= (uint64_t)c.hll_higher_precision_expansion_threshold ? 6 : 5);
+      void* sk = nullptr;
+      OCEAN_CUDA(cudaMallocAsync(&sk, std::max<uint64_t>(B->rows, 1) << log2p, s));
+      launch_hll_sketch_sample(a, b, h->w, log2p, 0u, (uint8_t*)sk, s);
+      if (learned) {
+        launch_hll_rows(a, h->w, log2p, 1.0, 0u, true, (const uint8_t*)sk, h->w.est, s);
+        MlpModel m = model_of(h);
+        if (!with_margin) m.margin = 0.f;
+        launch_mlp_estimate(m, row_inputs(h, b), a.rows, (uint32_t)c.esc_max_products, est, nullptr,
+                            &h->w.ctr->status, h->num_sms, s);
+      } else {
+        const double expansion = with_margin ? (log2p == 5 ? 2.0 : 1.5) * c.estimate_scale : 1.0;
+        launch_hll_rows(a, h->w, log2p, expansion, (uint32_t)c.esc_max_products, false, (const uint8_t*)sk, est, s);
+      }
+      const cudaError_t e = cudaGetLastError();
+      cudaFreeAsync(sk, s);
+      OCEAN_CUDA(e);
+      OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+      OCEAN_CUDA(cudaStreamSynchronize(s));
+      check_device_status(h);
+    };
+    if (A->rowptr_bits == 32) go(uint32_t{});
+    else go(uint64_t{});
+  });
+}
+
+int ocean_estimate_metrics(ocean_handle* h, const uint32_t* est, const uint32_t* truth, uint32_t min_products,
+                           double* out, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr, OCEAN_ERR_INVALID, "handle is NULL");
+    OCEAN_CHECK(out != nullptr, OCEAN_ERR_INVALID, "out is NULL");
+    const uint64_t n = h->w.rows;
+    OCEAN_CHECK(n == 0 || (est && truth), OCEAN_ERR_INVALID, "est or truth is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!h->metrics_dev) OCEAN_CUDA(cudaMalloc((void**)&h->metrics_dev, 8 * sizeof(double)));
+    OCEAN_CUDA(cudaMemsetAsync(h->metrics_dev, 0, 4 * sizeof(double), s));
+    SymPolicy sp;
+    NumPolicy np;
+    make_policies(h->cfg, &sp, &np);
+    MlpRowInputs in;
+    in.prod = h->w.prod;
+    in.lo = h->w.lo;
+    in.hi = h->w.hi;
+    launch_est_metrics(est, truth, in, n, np, min_products, h->metrics_dev, s);
+    double m[4];
+    OCEAN_CUDA(cudaMemcpyAsync(m, h->metrics_dev, sizeof m, cudaMemcpyDeviceToHost, s));
+    OCEAN_CUDA(cudaStreamSynchronize(s));
+    out[0] = m[1] > 0 ? m[0] / m[1] : 0.0;
+    out[1] = m[1] > 0 ? 100.0 * m[2] / m[1] : 0.0;
+    out[2] = m[1];
+    out[3] = m[3];
   });
 }
 

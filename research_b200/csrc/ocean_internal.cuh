@@ -73,7 +73,8 @@ struct DevCounters {
 enum DevError : unsigned int {
   DEV_TABLE_FULL = 1u,     // an open-addressing probe exceeded the table size
   DEV_BIN_OVERFLOW = 2u,   // a row did not fit the class it was placed in
-  DEV_COUNT_MISMATCH = 4u  // numeric output count differs from the symbolic count
+  DEV_COUNT_MISMATCH = 4u,  // numeric output count differs from the symbolic count
+  DEV_TC_TIMEOUT = 8u       // a tensor-core completion wait gave up (bounded spin)
 };
 
 constexpr uint32_t kUnknownCount = 0xFFFFFFFFu;

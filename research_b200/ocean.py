@@ -33,7 +33,13 @@ EXPORTS = (
     "ocean_create", "ocean_create_from_file", "ocean_destroy", "ocean_spgemm", "ocean_spgemm_host",
     "ocean_csr_free", "ocean_csr_download", "ocean_csr_download_rows", "ocean_symbolic", "ocean_stats_json", "ocean_stage_ms",
     "ocean_murmur3_u32", "ocean_last_error", "ocean_version", "ocean_symbolic_noalloc", "ocean_row_estimates",
+    "ocean_mlp_features", "ocean_mlp_forward", "ocean_mlp_grad", "ocean_mlp_adam", "ocean_mlp_builtin",
+    "ocean_estimate", "ocean_estimate_metrics",
 )
+
+MLP_FEATURES = 16
+MLP_PARAMS = 5313
+MLP_BLOB = 5346
 
 
 class OceanError(RuntimeError):
@@ -48,6 +54,13 @@ class CsrView(ctypes.Structure):
     _fields_ = [("rows", ctypes.c_uint64), ("cols", ctypes.c_uint64), ("nnz", ctypes.c_uint64),
                 ("rowptr", ctypes.c_void_p), ("rowptr_bits", ctypes.c_int32),
                 ("col", ctypes.c_void_p), ("val", ctypes.c_void_p)]
+
+
+class MlpModel(ctypes.Structure):
+    """ocean_mlp_model: device pointers of the parameters and the feature
+    normalisation, plus the log2 margin."""
+    _fields_ = [("params", ctypes.c_void_p), ("mu", ctypes.c_void_p), ("inv_sd", ctypes.c_void_p),
+                ("margin", ctypes.c_float)]
 
 
 class CsrOut(ctypes.Structure):
@@ -86,6 +99,14 @@ def lib() -> ctypes.CDLL:
     L.ocean_stage_ms.argtypes = [vp, ctypes.c_char_p]
     L.ocean_stage_ms.restype = ctypes.c_double
     L.ocean_murmur3_u32.argtypes = [vp, vp, u64, ctypes.c_uint32, vp]
+    f32 = ctypes.c_float
+    L.ocean_mlp_features.argtypes = [vp, P(CsrView), P(CsrView), vp, vp]
+    L.ocean_mlp_forward.argtypes = [vp, P(MlpModel), vp, u64, vp, vp]
+    L.ocean_mlp_grad.argtypes = [vp, P(MlpModel), vp, vp, u64, f32, vp, vp, vp]
+    L.ocean_mlp_adam.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, f32, f32, f32, f32, vp]
+    L.ocean_mlp_builtin.argtypes = [vp, ctypes.c_size_t]
+    L.ocean_estimate.argtypes = [vp, P(CsrView), P(CsrView), ctypes.c_int, ctypes.c_int, vp, vp]
+    L.ocean_estimate_metrics.argtypes = [vp, vp, vp, ctypes.c_uint32, vp, vp]
     L.ocean_last_error.restype = ctypes.c_char_p
     L.ocean_version.restype = ctypes.c_char_p
     for name in EXPORTS:
