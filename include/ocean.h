@@ -188,6 +188,41 @@ int ocean_estimate(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_vie
 int ocean_estimate_metrics(ocean_handle* h, const uint32_t* est, const uint32_t* truth, uint32_t min_products,
                            double* out, void* stream);
 
+/* ---- Batches ---------------------------------------------------------------
+ * Many independent products C[p] = A[p]·B[p] (B == NULL: C[p] = A[p]·A[p])
+ * computed as one block-diagonal product: the rows of all A[p] are stacked
+ * (their column ids shifted to the stacked B's rows), so every accumulator
+ * class runs once, as one persistent launch over the rows of all problems.
+ * No counterpart in the reference (one SpGEMM::run per product). */
+typedef struct ocean_batch ocean_batch;
+
+/* Plans a batch: stacks the problems, runs the pipeline once to size the
+ * class lists and buffers, and captures the pipeline (input stacking,
+ * analysis, estimation or exact counting, accumulators, row-pointer split)
+ * into a CUDA graph with no host synchronisation inside. With the config key
+ * "batch_autotune" the class policy (ESC limit, small-hash fill limit, bitmap
+ * span limits) is first searched on the batch by timing graph launches. The
+ * input device buffers and the handle must outlive the plan; their values may
+ * change between runs, their structure may not. */
+int ocean_batch_create(ocean_handle* h, uint64_t n, const ocean_csr_view* A, const ocean_csr_view* B,
+                       ocean_batch** out, void* stream);
+/* One run: a single graph launch on `stream`, then a wait and a check that the
+ * structure still matches the plan; C[0..n) receive views of the results
+ * (location 2: lent by the plan until its next run or destruction;
+ * ocean_csr_free on them only clears the struct). */
+int ocean_batch_run(ocean_batch* b, ocean_csr* C, void* stream);
+/* The graph launch alone, without waiting or checking. */
+int ocean_batch_launch(ocean_batch* b, void* stream);
+/* Views of the results of the last completed run (as ocean_batch_run). */
+int ocean_batch_results(ocean_batch* b, ocean_csr* C);
+/* Plan facts as JSON: sizes, workflow, estimator, kernels per run, tuned policy. */
+int ocean_batch_info_json(ocean_batch* b, char* buf, size_t cap, size_t* needed);
+int ocean_batch_destroy(ocean_batch* b);
+/* One-shot batch without a graph: C[p] are owned results that share one
+ * allocation, released when every C[p] has been passed to ocean_csr_free. */
+int ocean_spgemm_batched(ocean_handle* h, uint64_t n, const ocean_csr_view* A, const ocean_csr_view* B,
+                         ocean_csr* C, void* stream);
+
 /* Stats of the last multiply as JSON text, with the reference's keys
  * (kernels/SpGEMM.cuh:1788-1890: "A","B","C","stats","decision","timing",
  * "total_time","gflops", ...). If cap is too small, *needed gets the size. */

@@ -22,8 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
 
-LIB_SOURCES = ["kernels_core.cu", "segmentation.cu", "mlp.cu", "ocean_api.cu", "ocean_noalloc.cu"]
-HEADERS = ["ocean_internal.cuh", "kernels.h", "config.h", "mlp.h", "tc05.cuh", "mlp_weights.inc"]
+LIB_SOURCES = ["kernels_core.cu", "segmentation.cu", "mlp.cu", "batch.cu", "ocean_api.cu", "ocean_noalloc.cu"]
+HEADERS = ["ocean_internal.cuh", "kernels.h", "config.h", "mlp.h", "tc05.cuh", "mlp_weights.inc", "batch.h"]
 
 
 def nvcc() -> str:

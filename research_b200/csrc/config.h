@@ -195,6 +195,9 @@ struct Config {
   std::string learned_estimator_weights;  // weights file; empty: the built-in trained network
   double learned_margin_scale = 1.0;    // multiplies the network's log2 preallocation margin
   bool estimator_metrics = false;       // after an estimated multiply: error of the estimates vs exact counts
+  double hash_s_max_scale = 1.0;        // (0, 1]: fill limit of the small hash tables relative to the default
+  double bitmap_words_scale = 1.0;      // > 0: scales the column-span limits under which mid rows use bitmaps
+  bool batch_autotune = false;          // batched plans: search the class policy on the batch before capturing
 
   static Config from_json_text(const std::string& text) {
     Config c;
@@ -264,6 +267,9 @@ struct Config {
     gets("learned_estimator_weights", c.learned_estimator_weights);
     getd("learned_margin_scale", c.learned_margin_scale);
     getb("estimator_metrics", c.estimator_metrics);
+    getd("hash_s_max_scale", c.hash_s_max_scale);
+    getd("bitmap_words_scale", c.bitmap_words_scale);
+    getb("batch_autotune", c.batch_autotune);
     if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
     if (c.force_workflow < -1 || c.force_workflow > 2)

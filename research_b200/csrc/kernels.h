@@ -34,13 +34,21 @@ struct DevWork {
 constexpr int kScanTile = 4096;
 inline uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
 
+// Class choice of a row (tunable: the batched autotuner searches these).
+// Capacities of the fixed shared-memory tables bound the hash limits from above.
 struct SymPolicy {
-  uint32_t esc_max_products = 128;
-  int force_bin = -1;   // >= 0: every non-empty row goes to this class (tests)
+  uint32_t esc_max_products = 128;  // at most 128 (ESC4: 32 lanes x 4)
+  int force_bin = -1;               // >= 0: every non-empty row goes to this class (tests)
+  uint32_t hash_s_max = 1024;       // products of a small-hash row (table of 2048 slots)
+  uint32_t bm_words_m = 2048;       // 4096-product rows: bitmap when the span needs at most this many words
+  uint32_t bm_words_l = 8192;       // larger rows up to 16384 products: same rule
 };
 struct NumPolicy {
   uint32_t esc_max_products = 128;
   int force_bin = -1;
+  uint32_t hash_s_max = 512;        // outputs of a small-hash row (table of 1024 slots)
+  uint32_t bm_words_m = 1024;
+  uint32_t bm_words_l = 4096;
 };
 
 // Symbolic class of a row from its product count and output column span.
@@ -49,9 +57,9 @@ __device__ __forceinline__ int sym_bin_for(uint64_t p, uint64_t span, const SymP
   if (p <= pol.esc_max_products) return p <= 32 ? SB_ESC1 : (p <= 64 ? SB_ESC2 : SB_ESC4);
   const uint64_t words = (span + 63) >> 6;
   if (p > 16384) return SB_BITMAP;
-  if (p <= 1024) return SB_HASH_S;
-  if (p <= 4096) return (words <= 2048) ? SB_BITMAP : SB_HASH_M;
-  return (words <= 8192) ? SB_BITMAP : SB_HASH_L;
+  if (p <= pol.hash_s_max) return SB_HASH_S;
+  if (p <= 4096) return (words <= pol.bm_words_m) ? SB_BITMAP : SB_HASH_M;
+  return (words <= pol.bm_words_l) ? SB_BITMAP : SB_HASH_L;
 }
 
 // Numeric class of a row from its exact output count.
@@ -61,9 +69,9 @@ __device__ __forceinline__ int num_bin_for(uint32_t n, uint64_t p, uint64_t span
   if (pol.force_bin >= 0) return pol.force_bin;
   if (p <= pol.esc_max_products) return p <= 32 ? NB_ESC1 : (p <= 64 ? NB_ESC2 : NB_ESC4);
   const uint64_t words = (span + 63) >> 6;
-  if (n <= 512) return NB_HASH_S;
-  if (n <= 2048) return (words <= 1024) ? NB_BITMAP : NB_HASH_M;
-  if (n <= 4096) return (words <= 4096) ? NB_BITMAP : NB_HASH_L;
+  if (n <= pol.hash_s_max) return NB_HASH_S;
+  if (n <= 2048) return (words <= pol.bm_words_m) ? NB_BITMAP : NB_HASH_M;
+  if (n <= 4096) return (words <= pol.bm_words_l) ? NB_BITMAP : NB_HASH_L;
   return NB_BITMAP;
 }
 
@@ -101,9 +109,10 @@ int launch_hll_rows(const Csr<RP>& A, const DevWork& w, int log2p, double expans
                     const uint8_t* sketch, uint32_t* out, cudaStream_t s);
 
 // Estimation workflow epilogue: copy the rows that fit their estimate from the
-// temporary output into C.
+// temporary output into C. stop (optional): the kernel does nothing if
+// DEV_BATCH_MISMATCH is set there.
 void launch_copy_rows(const DevWork& w, const uint32_t* t_col, const double* t_val, uint32_t* c_col,
-                      double* c_val, cudaStream_t s);
+                      double* c_val, cudaStream_t s, const unsigned* stop = nullptr);
 
 // Exact counts (bitmap symbolic kernel) and exact numeric output (bitmap
 // numeric kernel) for the rows of the overflow queue.

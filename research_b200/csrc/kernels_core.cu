@@ -1273,7 +1273,8 @@ __global__ void __launch_bounds__(256) k_copy_rows(uint64_t rows, const uint64_t
                                                    const uint64_t* __restrict__ dst_off,
                                                    const uint32_t* __restrict__ t_col,
                                                    const double* __restrict__ t_val, uint32_t* __restrict__ c_col,
-                                                   double* __restrict__ c_val) {
+                                                   double* __restrict__ c_val, const unsigned* __restrict__ stop) {
+  if (stop && (*stop & DEV_BATCH_MISMATCH)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint64_t r = (uint64_t)blockIdx.x * 8 + warp; r < rows; r += (uint64_t)gridDim.x * 8) {
     const uint32_t n = cnt[r];
@@ -1504,10 +1505,10 @@ int launch_hll_rows(const Csr<RP>& A, const DevWork& w, int log2p, double expans
 }
 
 void launch_copy_rows(const DevWork& w, const uint32_t* t_col, const double* t_val, uint32_t* c_col, double* c_val,
-                      cudaStream_t s) {
+                      cudaStream_t s, const unsigned* stop) {
   if (w.rows == 0) return;
   const unsigned g = (unsigned)std::min<uint64_t>((w.rows + 7) / 8, 148u * 64u);
-  k_copy_rows<<<g, 256, 0, s>>>(w.rows, w.est_off, w.est, w.cnt, w.rowptr64, t_col, t_val, c_col, c_val);
+  k_copy_rows<<<g, 256, 0, s>>>(w.rows, w.est_off, w.est, w.cnt, w.rowptr64, t_col, t_val, c_col, c_val, stop);
 }
 
 template <typename RP>

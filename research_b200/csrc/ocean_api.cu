@@ -12,11 +12,13 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <string>
 #include <vector>
 
 #include "config.h"
+#include "batch.h"
 #include "kernels.h"
 #include "mlp.h"
 #include "ocean.h"
@@ -54,6 +56,8 @@ struct CResult {
   void* rowptr = nullptr;
   uint32_t* col = nullptr;
   double* val = nullptr;
+  int refs = 1;  // results of one batched call share one allocation
+  bool plain_alloc = false;  // allocated with cudaMalloc (freed with cudaFree)
 };
 
 enum Ev {
@@ -220,16 +224,20 @@ void init_handle(ocean_handle* h, const std::string& json) {
   OCEAN_CUDA(cudaMalloc((void**)&h->w.ctr, sizeof(DevCounters)));
 }
 
-void ensure_rows(ocean_handle* h, uint64_t rows) {
-  if (rows <= h->cap_rows && h->w.prod) {
-    h->w.rows = rows;
-    return;
-  }
-  DevWork& x = h->w;
+// Frees the per-row arrays of a DevWork (not its counters).
+void free_work_rows(DevWork& x) {
   void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.maxb, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
                 x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf};
   for (void* p : ps)
     if (p) cudaFree(p);
+  DevCounters* keep = x.ctr;
+  x = DevWork();
+  x.ctr = keep;
+}
+
+// Per-row arrays of a DevWork for `rows` rows of A (about 100 B per row).
+void alloc_work_rows(DevWork& x, uint64_t rows) {
+  free_work_rows(x);
   const uint64_t r = std::max<uint64_t>(rows, 1);
   OCEAN_CUDA(cudaMalloc((void**)&x.prod, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.anz, r * 4));
@@ -247,8 +255,17 @@ void ensure_rows(ocean_handle* h, uint64_t rows) {
   OCEAN_CUDA(cudaMalloc((void**)&x.est_off, (r + 1) * 8));
   OCEAN_CUDA(cudaMalloc((void**)&x.cnt, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.ovf, r * 4));
-  h->cap_rows = r;
   x.rows = rows;
+}
+
+void ensure_rows(ocean_handle* h, uint64_t rows) {
+  if (rows <= h->cap_rows && h->w.prod) {
+    h->w.rows = rows;
+    return;
+  }
+  h->cap_rows = 0;
+  alloc_work_rows(h->w, rows);
+  h->cap_rows = std::max<uint64_t>(rows, 1);
 }
 
 void validate_view(const ocean_csr_view* m, const char* name) {
@@ -330,10 +347,24 @@ uint64_t available_device_bytes(int device) {
 
 // Policies of the class choice from the config.
 void make_policies(const Config& c, SymPolicy* sp, NumPolicy* np) {
+  OCEAN_CHECK(c.esc_max_products >= 0 && c.esc_max_products <= 128, OCEAN_ERR_INVALID,
+              "esc_max_products must be in [0, 128]");
+  OCEAN_CHECK(c.hash_s_max_scale > 0.0 && c.hash_s_max_scale <= 1.0, OCEAN_ERR_INVALID,
+              "hash_s_max_scale must be in (0, 1]");
+  OCEAN_CHECK(c.bitmap_words_scale > 0.0 && c.bitmap_words_scale <= 64.0, OCEAN_ERR_INVALID,
+              "bitmap_words_scale must be in (0, 64]");
+  *sp = SymPolicy();
+  *np = NumPolicy();
   sp->esc_max_products = (uint32_t)c.esc_max_products;
   sp->force_bin = c.force_sym_bin;
   np->esc_max_products = (uint32_t)c.esc_max_products;
   np->force_bin = c.force_num_bin;
+  sp->hash_s_max = std::max<uint32_t>(1, (uint32_t)(sp->hash_s_max * c.hash_s_max_scale));
+  np->hash_s_max = std::max<uint32_t>(1, (uint32_t)(np->hash_s_max * c.hash_s_max_scale));
+  sp->bm_words_m = (uint32_t)(sp->bm_words_m * c.bitmap_words_scale);
+  sp->bm_words_l = (uint32_t)(sp->bm_words_l * c.bitmap_words_scale);
+  np->bm_words_m = (uint32_t)(np->bm_words_m * c.bitmap_words_scale);
+  np->bm_words_l = (uint32_t)(np->bm_words_l * c.bitmap_words_scale);
   OCEAN_CHECK(sp->force_bin < SB_COUNT && np->force_bin < NB_COUNT, OCEAN_ERR_INVALID, "forced class out of range");
 }
 
@@ -476,14 +507,14 @@ MlpModel model_of(const ocean_handle* h) {
 // The estimator's per-row inputs: the analysis arrays, the raw HLL estimates
 // in w.est, and two scalars of B.
 template <typename RP>
-MlpRowInputs row_inputs(const ocean_handle* h, const Csr<RP>& B) {
+MlpRowInputs row_inputs(const DevWork& w, const Csr<RP>& B) {
   MlpRowInputs in;
-  in.anz = h->w.anz;
-  in.prod = h->w.prod;
-  in.lo = h->w.lo;
-  in.hi = h->w.hi;
-  in.maxb = h->w.maxb;
-  in.hll = h->w.est;
+  in.anz = w.anz;
+  in.prod = w.prod;
+  in.lo = w.lo;
+  in.hi = w.hi;
+  in.maxb = w.maxb;
+  in.hll = w.est;
   in.log_b_cols = log2f(1.f + (float)B.cols);
   in.log_b_avg = log2f(1.f + (B.rows ? (float)((double)B.nnz / (double)B.rows) : 0.f));
   return in;
@@ -558,7 +589,7 @@ int choose_workflow(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStr
       if (learned) {
         // raw HLL estimates become a feature; the network then writes the estimates over them
         h->st.launches += launch_hll_rows(A, h->w, log2p, 1.0, 0u, true, (const uint8_t*)sk, h->w.est, s);
-        h->st.launches += launch_mlp_estimate(model_of(h), row_inputs(h, B), A.rows, (uint32_t)c.esc_max_products,
+        h->st.launches += launch_mlp_estimate(model_of(h), row_inputs(h->w, B), A.rows, (uint32_t)c.esc_max_products,
                                               h->w.est, raw, &h->w.ctr->status, h->num_sms, s);
         h->st.estimator = 2;
       } else {
@@ -584,7 +615,7 @@ template <typename RP>
 void measure_estimates(ocean_handle* h, const Csr<RP>& B, const NumPolicy& np, cudaStream_t s) {
   if (!h->metrics_dev) OCEAN_CUDA(cudaMalloc((void**)&h->metrics_dev, 8 * sizeof(double)));
   OCEAN_CUDA(cudaMemsetAsync(h->metrics_dev, 0, 8 * sizeof(double), s));
-  const MlpRowInputs in = row_inputs(h, B);
+  const MlpRowInputs in = row_inputs(h->w, B);
   launch_est_metrics(h->w.est, h->w.cnt, in, h->w.rows, np, 0u, h->metrics_dev, s);
   launch_est_metrics(h->raw_est, h->w.cnt, in, h->w.rows, np, 0u, h->metrics_dev + 4, s);
   h->st.launches += 2;
@@ -955,6 +986,427 @@ void with_status(ocean_handle* h, cudaStream_t s, F&& launch) {
 }
 }  // namespace
 
+// ---------------------------------------------------------------- batches
+// A batch plan: many independent products C_p = A_p * B_p run as one
+// block-diagonal product (see batch.cu). Planning stacks the inputs, runs the
+// whole pipeline once with read-backs to learn the class sizes, the
+// temporary and output sizes, and captures the same pipeline, without any
+// read-back or allocation, into a CUDA graph; every run is then one graph
+// launch. The plan owns its per-row arrays and counters, so calls on the
+// handle in between do not disturb it; the handle (and the inputs' device
+// buffers) must outlive the plan. The inputs' values (and columns) may change
+// between runs; a run whose structure no longer matches the plan fails.
+struct ocean_batch {
+  ocean_handle* h = nullptr;
+  Config cfg;  // the handle's config plus the tuned class policy
+  uint32_t n = 0;
+  bool same_b = false;  // every B_p is A_p: the stacked B shares A's row pointers and values
+  int bits = 32;        // stacked input row-pointer width
+  uint64_t rows = 0, nnz = 0, brows = 0, bnnz = 0, bcols = 0;
+  std::vector<uint64_t> row0, nnz0, brow0, bnnz0;  // n + 1 prefixes
+  std::vector<uint64_t> a_rows, b_cols;
+  BatchProblem* d_probs = nullptr;
+  uint64_t* d_pref = nullptr;  // row0 | nnz0 | brow0 | bnnz0 | out0 (n + 1 each)
+  void* a_rp = nullptr;
+  uint32_t* a_col = nullptr;
+  double* a_val = nullptr;
+  void* b_rp = nullptr;
+  uint32_t* b_col = nullptr;
+  double* b_val = nullptr;
+  DevWork w;
+  int wf = 0;         // Workflow
+  int estimator = 0;  // 0 products, 1 HLL, 2 learned
+  int log2p = 5;
+  double expansion = 1.0;
+  uint8_t* sketch = nullptr;
+  unsigned sym_counts[SB_COUNT] = {0};
+  unsigned num_counts[NB_COUNT] = {0};
+  uint64_t total_est = 0, c_nnz = 0;
+  int out_bits = 32;
+  uint32_t* t_col = nullptr;
+  double* t_val = nullptr;
+  uint32_t* c_col = nullptr;
+  double* c_val = nullptr;
+  void* c_rp = nullptr;  // rows + n per-problem row pointers
+  std::vector<uint64_t> c_off;  // n + 1 starts in the stacked C
+  uint64_t* d_bounds = nullptr;  // the same, written by every run
+  std::vector<uint64_t> h_bounds;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;  // kernels per run
+  double tuned_ms = 0.0;
+  std::string tuning;  // description of the tuned policy
+  DevCounters* h_ctr = nullptr;
+
+  uint64_t* pref(int i) const { return d_pref + (uint64_t)i * (n + 1); }
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  void free_arenas() {
+    for (void* p : {(void*)t_col, (void*)t_val, (void*)c_col, (void*)c_val, (void*)c_rp})
+      if (p) cudaFree(p);
+    t_col = nullptr, t_val = nullptr, c_col = nullptr, c_val = nullptr, c_rp = nullptr;
+  }
+  ~ocean_batch() {
+    drop_graph();
+    free_arenas();
+    free_work_rows(w);
+    for (void* p : {(void*)w.ctr, (void*)d_probs, (void*)d_pref, a_rp, (void*)a_col, (void*)a_val, (void*)sketch,
+                    (void*)d_bounds})
+      if (p) cudaFree(p);
+    if (!same_b)
+      for (void* p : {b_rp, (void*)b_col, (void*)b_val})
+        if (p) cudaFree(p);
+    else if (b_col)
+      cudaFree(b_col);
+    if (h_ctr) cudaFreeHost(h_ctr);
+  }
+};
+
+namespace {
+
+void batch_readback(ocean_batch* b, cudaStream_t s) {
+  OCEAN_CUDA(cudaMemcpyAsync(b->h_ctr, b->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+  OCEAN_CUDA(cudaStreamSynchronize(s));
+  if (b->h_ctr->status) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "%s (status 0x%x, batched)", status_text(b->h_ctr->status), b->h_ctr->status);
+    throw OceanError{(b->h_ctr->status & DEV_TC_TIMEOUT) ? (int)OCEAN_ERR_TIMEOUT : (int)OCEAN_ERR_CAPACITY, buf};
+  }
+}
+
+// The whole batched pipeline on stream s. plan = true: with read-backs that
+// fix the workflow, class sizes and buffer sizes (and allocate the arenas);
+// plan = false: the same launches with those values, nothing else (capturable).
+template <typename RP>
+void batch_pipeline(ocean_batch* b, cudaStream_t s, bool plan) {
+  ocean_handle* h = b->h;
+  DevWork& w = b->w;
+  const uint32_t n = b->n;
+  SymPolicy sp;
+  NumPolicy np;
+  make_policies(b->cfg, &sp, &np);
+  int launched = 0;
+  // 1. stacked inputs
+  launch_batch_rowptr<RP>(b->d_probs, b->pref(0), n, b->rows, b->nnz, false, (RP*)b->a_rp, s);
+  launch_batch_entries(b->d_probs, b->pref(1), n, b->nnz, false, b->a_col, b->a_val, s);
+  launched += 2;
+  if (b->same_b) {
+    launch_batch_entries(b->d_probs, b->pref(1), n, b->nnz, true, b->b_col, nullptr, s);
+    launched += 1;
+  } else {
+    launch_batch_rowptr<RP>(b->d_probs, b->pref(2), n, b->brows, b->bnnz, true, (RP*)b->b_rp, s);
+    launch_batch_entries(b->d_probs, b->pref(3), n, b->bnnz, true, b->b_col, b->b_val, s);
+    launched += 2;
+  }
+  Csr<RP> A, B;
+  A.rows = b->rows, A.cols = b->brows, A.nnz = b->nnz, A.rp = (const RP*)b->a_rp, A.col = b->a_col, A.val = b->a_val;
+  B.rows = b->brows, B.cols = b->bcols, B.nnz = b->bnnz, B.rp = (const RP*)b->b_rp, B.col = b->b_col,
+  B.val = b->b_val;
+  // 2. analysis
+  w.bm_cache = nullptr;
+  w.bm_cache_words = 0;
+  OCEAN_CUDA(cudaMemsetAsync(w.ctr, 0, sizeof(DevCounters), s));
+  launched += launch_analysis(A, B, w, sp, s);
+  if (plan) {
+    batch_readback(b, s);
+    const DevCounters& k = *b->h_ctr;
+    for (int i = 0; i < SB_COUNT; ++i) b->sym_counts[i] = k.sym_count[i];
+    const Config& c = b->cfg;
+    const double avg = A.rows ? (double)k.total_products / (double)A.rows : 0.0;
+    if (c.force_workflow == WF_PRECISE) b->wf = WF_PRECISE;
+    else if (c.use_learned_estimator || c.force_workflow == WF_ESTIMATION) b->wf = WF_ESTIMATION;
+    else if (c.force_workflow == WF_ULTRASPARSE || (c.use_ultrasparse_workflow && avg <= c.usparse_avg_product_threshold))
+      b->wf = WF_ULTRASPARSE;
+    else b->wf = WF_PRECISE;
+    b->estimator = b->wf == WF_ESTIMATION ? (c.use_learned_estimator ? 2 : 1) : 0;
+    if (b->estimator == 2) load_model(h);
+    const uint64_t ratio = A.nnz ? k.total_products / A.nnz : 0;
+    b->log2p = b->estimator == 2 ? kLearnedLog2p : (ratio >= (uint64_t)c.hll_higher_precision_expansion_threshold ? 6 : 5);
+    b->expansion = (b->log2p == 5 ? 2.0 : 1.5) * c.estimate_scale;
+    if (b->estimator && !b->sketch) OCEAN_CUDA(cudaMalloc((void**)&b->sketch, std::max<uint64_t>(B.rows, 1) << 6));
+  }
+  if (b->wf == WF_PRECISE) {
+    launched += launch_symbolic(A, B, w, h->num_sms, s, nullptr, b->sym_counts);
+    launched += launch_scan(w, w.row_nnz, w.rowptr64, w.rowptr32, &w.ctr->total_nnz, true, np, s);
+    if (plan) {
+      batch_readback(b, s);
+      b->c_nnz = b->h_ctr->total_nnz;
+      for (int i = 0; i < NB_COUNT; ++i) b->num_counts[i] = b->h_ctr->num_count[i];
+    } else {
+      launch_batch_guard(w.ctr, &w.ctr->total_nnz, b->c_nnz, s);
+      launched += 1;
+    }
+  } else {
+    if (b->wf == WF_ULTRASPARSE) {
+      OCEAN_CUDA(cudaMemcpyAsync(w.est, w.prod, A.rows * 4, cudaMemcpyDeviceToDevice, s));
+    } else {
+      launched += launch_hll_sketch_sample(A, B, w, b->log2p, 0u, b->sketch, s);
+      if (b->estimator == 2) {
+        launched += launch_hll_rows(A, w, b->log2p, 1.0, 0u, true, b->sketch, w.est, s);
+        launched += launch_mlp_estimate(model_of(h), row_inputs(w, B), A.rows, sp.esc_max_products, w.est, nullptr,
+                                        &w.ctr->status, h->num_sms, s);
+      } else {
+        launched += launch_hll_rows(A, w, b->log2p, b->expansion, sp.esc_max_products, false, b->sketch, w.est, s);
+      }
+    }
+    launched += launch_scan(w, w.est, w.est_off, nullptr, &w.ctr->total_est, true, np, s);
+    if (plan) {
+      batch_readback(b, s);
+      b->total_est = b->h_ctr->total_est;
+      for (int i = 0; i < NB_COUNT; ++i) b->num_counts[i] = b->h_ctr->num_count[i];
+      OCEAN_CUDA(cudaMalloc((void**)&b->t_col, std::max<uint64_t>(b->total_est, 1) * 4));
+      OCEAN_CUDA(cudaMalloc((void**)&b->t_val, std::max<uint64_t>(b->total_est, 1) * 8));
+    } else {
+      launch_batch_guard(w.ctr, &w.ctr->total_est, b->total_est, s);
+      launched += 1;
+    }
+    OCEAN_CUDA(cudaMemsetAsync(w.cnt, 0, A.rows * 4, s));
+    const OutSpec est_out{w.est_off, w.est, w.cnt, w.ovf, &w.ctr->overflow_n};
+    launched += launch_numeric(A, B, w, est_out, b->t_col, b->t_val, h->num_sms, s, nullptr, b->num_counts);
+    launched += launch_overflow(A, B, w, false, nullptr, nullptr, h->num_sms, s);
+    launched += launch_scan(w, w.cnt, w.rowptr64, w.rowptr32, &w.ctr->total_nnz, false, np, s);
+    if (plan) {
+      batch_readback(b, s);
+      b->c_nnz = b->h_ctr->total_nnz;
+    } else {
+      launch_batch_guard(w.ctr, &w.ctr->total_nnz, b->c_nnz, s);
+      launched += 1;
+    }
+  }
+  if (plan) {
+    b->out_bits = b->c_nnz >= (1ull << 32) ? 64 : 32;
+    OCEAN_CUDA(cudaMalloc((void**)&b->c_col, std::max<uint64_t>(b->c_nnz, 1) * 4));
+    OCEAN_CUDA(cudaMalloc((void**)&b->c_val, std::max<uint64_t>(b->c_nnz, 1) * 8));
+    OCEAN_CUDA(cudaMalloc(&b->c_rp, (b->rows + n) * (b->out_bits / 8)));
+  }
+  if (b->wf == WF_PRECISE) {
+    const OutSpec exact{w.rowptr64, w.row_nnz, nullptr, nullptr, nullptr};
+    launched += launch_numeric(A, B, w, exact, b->c_col, b->c_val, h->num_sms, s, nullptr, b->num_counts);
+  } else {
+    launch_copy_rows(w, b->t_col, b->t_val, b->c_col, b->c_val, s, &w.ctr->status);
+    launched += 1;
+    launched += launch_overflow(A, B, w, true, b->c_col, b->c_val, h->num_sms, s);
+  }
+  // 3. one row-pointer array per problem
+  if (b->out_bits == 64) launch_batch_rebase<uint64_t, uint64_t>(w.rowptr64, b->pref(0), b->pref(4), n, b->rows + n,
+                                                                 (uint64_t*)b->c_rp, s);
+  else launch_batch_rebase<uint64_t, uint32_t>(w.rowptr64, b->pref(0), b->pref(4), n, b->rows + n,
+                                               (uint32_t*)b->c_rp, s);
+  launch_batch_bounds<uint64_t>(w.rowptr64, b->pref(0), n, b->d_bounds, s);
+  launched += 2;
+  OCEAN_CUDA(cudaGetLastError());
+  if (plan) {
+    b->c_off.assign(n + 1, 0);
+    OCEAN_CUDA(cudaMemcpyAsync(b->c_off.data(), b->d_bounds, (n + 1) * 8, cudaMemcpyDeviceToHost, s));
+    batch_readback(b, s);
+    b->launches = launched + (b->wf == WF_PRECISE ? 1 : 2);  // the capacity guards of a captured run
+  }
+}
+
+void batch_run_pipeline(ocean_batch* b, cudaStream_t s, bool plan) {
+  if (b->bits == 32) batch_pipeline<uint32_t>(b, s, plan);
+  else batch_pipeline<uint64_t>(b, s, plan);
+}
+
+// Plans (eager run), then captures the pipeline into a graph.
+void batch_plan_and_capture(ocean_batch* b, cudaStream_t s) {
+  b->drop_graph();
+  b->free_arenas();
+  if (b->rows == 0) {  // every problem is empty: row pointers of zeros
+    b->out_bits = 32;
+    b->c_nnz = 0;
+    b->c_off.assign(b->n + 1, 0);
+    OCEAN_CUDA(cudaMalloc(&b->c_rp, b->n * 4ull));
+    OCEAN_CUDA(cudaMemset(b->c_rp, 0, b->n * 4ull));
+    return;
+  }
+  batch_run_pipeline(b, s, true);
+  cudaStream_t cs;
+  OCEAN_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    try {
+      batch_run_pipeline(b, cs, false);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(cs, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaStreamDestroy(cs);
+      throw;
+    }
+    e = cudaStreamEndCapture(cs, &b->graph);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  cudaStreamDestroy(cs);
+  OCEAN_CUDA(e);
+}
+
+// One graph launch; with check, waits and verifies the structure still matches.
+void batch_launch(ocean_batch* b, cudaStream_t s, bool check) {
+  if (!b->exec) return;
+  OCEAN_CUDA(cudaGraphLaunch(b->exec, s));
+  if (check) {
+    b->h_bounds.resize(b->n + 1);
+    OCEAN_CUDA(cudaMemcpyAsync(b->h_bounds.data(), b->d_bounds, (b->n + 1) * 8, cudaMemcpyDeviceToHost, s));
+    OCEAN_CUDA(cudaMemcpyAsync(b->h_ctr, b->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+    OCEAN_CUDA(cudaStreamSynchronize(s));
+    const unsigned st = b->h_ctr->status;
+    OCEAN_CHECK(!(st & DEV_BATCH_MISMATCH) && b->h_bounds == b->c_off &&
+                    (b->wf == WF_PRECISE || b->h_ctr->total_est == b->total_est),
+                OCEAN_ERR_INVALID, "batch structure changed since the plan was made (re-plan it)");
+    batch_readback(b, s);
+  }
+}
+
+// Coordinate search over the class policy on the batch itself: each candidate
+// is planned, captured and timed over `reps` graph launches (CUDA events);
+// the fastest is kept.
+void batch_autotune(ocean_batch* b, cudaStream_t s, int reps) {
+  struct Knob {
+    const char* name;
+    std::vector<double> values;
+  };
+  std::vector<Knob> knobs = {{"esc_max_products", {128, 64, 32}},
+                             {"hash_s_max_scale", {1.0, 0.75, 0.5}},
+                             {"bitmap_words_scale", {1.0, 0.5, 2.0, 4.0}}};
+  cudaEvent_t e0, e1;
+  OCEAN_CUDA(cudaEventCreate(&e0));
+  OCEAN_CUDA(cudaEventCreate(&e1));
+  auto set = [&](const char* k, double v) {
+    if (!strcmp(k, "esc_max_products")) b->cfg.esc_max_products = (int)v;
+    else if (!strcmp(k, "hash_s_max_scale")) b->cfg.hash_s_max_scale = v;
+    else b->cfg.bitmap_words_scale = v;
+  };
+  auto get = [&](const char* k) -> double {
+    if (!strcmp(k, "esc_max_products")) return b->cfg.esc_max_products;
+    if (!strcmp(k, "hash_s_max_scale")) return b->cfg.hash_s_max_scale;
+    return b->cfg.bitmap_words_scale;
+  };
+  auto measure = [&]() -> double {
+    batch_plan_and_capture(b, s);
+    batch_launch(b, s, true);  // warm-up and structure check
+    OCEAN_CUDA(cudaEventRecord(e0, s));
+    for (int i = 0; i < reps; ++i) OCEAN_CUDA(cudaGraphLaunch(b->exec, s));
+    OCEAN_CUDA(cudaEventRecord(e1, s));
+    OCEAN_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    OCEAN_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    return ms / reps;
+  };
+  double best = measure();
+  for (const Knob& k : knobs) {
+    double keep = get(k.name);
+    for (double v : k.values) {
+      if (v == keep) continue;
+      set(k.name, v);
+      const double t = measure();
+      if (t < best) best = t, keep = v;
+    }
+    set(k.name, keep);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  batch_plan_and_capture(b, s);
+  b->tuned_ms = best;
+  char buf[160];
+  snprintf(buf, sizeof buf, "esc_max_products=%d hash_s_max_scale=%g bitmap_words_scale=%g", b->cfg.esc_max_products,
+           b->cfg.hash_s_max_scale, b->cfg.bitmap_words_scale);
+  b->tuning = buf;
+}
+
+// Stacks the problems' geometry and copies the problem table to the device.
+void batch_setup(ocean_batch* b, uint64_t n, const ocean_csr_view* A, const ocean_csr_view* B) {
+  OCEAN_CHECK(n > 0 && n < 0xFFFFFFFFull, OCEAN_ERR_INVALID, "batch size must be in [1, 2^32)");
+  OCEAN_CHECK(A != nullptr, OCEAN_ERR_INVALID, "A is NULL");
+  b->n = (uint32_t)n;
+  b->same_b = true;
+  for (uint64_t p = 0; p < n; ++p) {
+    validate_view(&A[p], "A[p]");
+    if (B) {
+      validate_view(&B[p], "B[p]");
+      OCEAN_CHECK(A[p].cols == B[p].rows, OCEAN_ERR_INVALID, "Incompatible matrix dimensions (A[p].cols != B[p].rows)");
+      if (memcmp(&A[p], &B[p], sizeof(ocean_csr_view)) != 0) b->same_b = false;
+    } else {
+      OCEAN_CHECK(A[p].cols == A[p].rows, OCEAN_ERR_INVALID, "B = NULL needs square A[p] (C = A[p] * A[p])");
+    }
+  }
+  b->row0.assign(n + 1, 0), b->nnz0.assign(n + 1, 0), b->brow0.assign(n + 1, 0), b->bnnz0.assign(n + 1, 0);
+  b->a_rows.resize(n), b->b_cols.resize(n);
+  std::vector<BatchProblem> probs(n);
+  for (uint64_t p = 0; p < n; ++p) {
+    const ocean_csr_view& a = A[p];
+    const ocean_csr_view& bb = B ? B[p] : A[p];
+    b->row0[p + 1] = b->row0[p] + a.rows;
+    b->nnz0[p + 1] = b->nnz0[p] + a.nnz;
+    b->brow0[p + 1] = b->brow0[p] + bb.rows;
+    b->bnnz0[p + 1] = b->bnnz0[p] + bb.nnz;
+    b->a_rows[p] = a.rows;
+    b->b_cols[p] = bb.cols;
+    b->bcols = std::max<uint64_t>(b->bcols, bb.cols);
+    BatchProblem& q = probs[p];
+    q.a_rp = a.rowptr, q.a_col = a.col, q.a_val = a.val, q.a_bits = (uint32_t)a.rowptr_bits;
+    q.b_rp = bb.rowptr, q.b_col = bb.col, q.b_val = bb.val, q.b_bits = (uint32_t)bb.rowptr_bits;
+    q.nnz0 = b->nnz0[p], q.brow0 = b->brow0[p], q.bnnz0 = b->bnnz0[p];
+  }
+  b->rows = b->row0[n], b->nnz = b->nnz0[n], b->brows = b->brow0[n], b->bnnz = b->bnnz0[n];
+  OCEAN_CHECK(b->rows < 0xFFFFFFFFull && b->brows < 0xFFFFFFFFull, OCEAN_ERR_INVALID,
+              "the stacked batch has 2^32 - 1 or more rows");
+  b->bits = (b->nnz >= (1ull << 32) || b->bnnz >= (1ull << 32)) ? 64 : 32;
+  const int rb = b->bits / 8;
+  OCEAN_CUDA(cudaMalloc((void**)&b->d_probs, n * sizeof(BatchProblem)));
+  OCEAN_CUDA(cudaMemcpy(b->d_probs, probs.data(), n * sizeof(BatchProblem), cudaMemcpyHostToDevice));
+  std::vector<uint64_t> pref(5 * (n + 1));
+  for (uint64_t p = 0; p <= n; ++p) {
+    pref[p] = b->row0[p];
+    pref[(n + 1) + p] = b->nnz0[p];
+    pref[2 * (n + 1) + p] = b->brow0[p];
+    pref[3 * (n + 1) + p] = b->bnnz0[p];
+    pref[4 * (n + 1) + p] = b->row0[p] + p;
+  }
+  OCEAN_CUDA(cudaMalloc((void**)&b->d_pref, pref.size() * 8));
+  OCEAN_CUDA(cudaMemcpy(b->d_pref, pref.data(), pref.size() * 8, cudaMemcpyHostToDevice));
+  OCEAN_CUDA(cudaMalloc(&b->a_rp, (b->rows + 1) * rb));
+  OCEAN_CUDA(cudaMalloc((void**)&b->a_col, std::max<uint64_t>(b->nnz, 1) * 4));
+  OCEAN_CUDA(cudaMalloc((void**)&b->a_val, std::max<uint64_t>(b->nnz, 1) * 8));
+  if (b->same_b) {
+    b->b_rp = b->a_rp;
+    b->b_val = b->a_val;
+    OCEAN_CUDA(cudaMalloc((void**)&b->b_col, std::max<uint64_t>(b->nnz, 1) * 4));
+  } else {
+    OCEAN_CUDA(cudaMalloc(&b->b_rp, (b->brows + 1) * rb));
+    OCEAN_CUDA(cudaMalloc((void**)&b->b_col, std::max<uint64_t>(b->bnnz, 1) * 4));
+    OCEAN_CUDA(cudaMalloc((void**)&b->b_val, std::max<uint64_t>(b->bnnz, 1) * 8));
+  }
+  OCEAN_CUDA(cudaMalloc((void**)&b->w.ctr, sizeof(DevCounters)));
+  OCEAN_CUDA(cudaMalloc((void**)&b->d_bounds, (n + 1) * 8));
+  OCEAN_CUDA(cudaHostAlloc((void**)&b->h_ctr, sizeof(DevCounters), cudaHostAllocDefault));
+  alloc_work_rows(b->w, b->rows);
+}
+
+// The n results as views into the plan's arena (location 2: lent by the plan).
+void batch_outputs(const ocean_batch* b, ocean_csr* C) {
+  for (uint32_t p = 0; p < b->n; ++p) {
+    ocean_csr& c = C[p];
+    std::memset(&c, 0, sizeof c);
+    c.rows = b->a_rows[p];
+    c.cols = b->b_cols[p];
+    c.rowptr_bits = b->out_bits;
+    c.location = 2;
+    c.rowptr = (char*)b->c_rp + (b->row0[p] + p) * (uint64_t)(b->out_bits / 8);
+    c.nnz = b->c_off[p + 1] - b->c_off[p];
+    if (c.nnz) {
+      c.col = b->c_col + b->c_off[p];
+      c.val = b->c_val + b->c_off[p];
+    }
+  }
+}
+
+}  // namespace
+
 extern "C" {
 
 int ocean_create(ocean_handle** out, const char* json_config) {
@@ -1066,11 +1518,13 @@ int ocean_csr_free(ocean_csr* C, void* stream) {
   return guarded([&] {
     OCEAN_CHECK(C != nullptr, OCEAN_ERR_INVALID, "C is NULL");
     CResult* o = (CResult*)C->_owner;
-    if (o && o->location == 0) {
+    if (o && o->location == 0 && --o->refs == 0) {
       cudaStream_t s = (cudaStream_t)stream;
-      OCEAN_CUDA(cudaFreeAsync(o->rowptr, s));
-      OCEAN_CUDA(cudaFreeAsync(o->col, s));
-      OCEAN_CUDA(cudaFreeAsync(o->val, s));
+      for (void* p : {o->rowptr, (void*)o->col, (void*)o->val}) {
+        if (!p) continue;
+        if (o->plain_alloc) OCEAN_CUDA(cudaFree(p));
+        else OCEAN_CUDA(cudaFreeAsync(p, s));
+      }
       delete o;
     }
     std::memset(C, 0, sizeof(*C));
@@ -1195,7 +1649,7 @@ int ocean_mlp_features(ocean_handle* h, const ocean_csr_view* A, const ocean_csr
       OCEAN_CUDA(cudaMallocAsync(&sk, std::max<uint64_t>(B->rows, 1) << kLearnedLog2p, s));
       launch_hll_sketch_sample(a, b, h->w, kLearnedLog2p, 0u, (uint8_t*)sk, s);
       launch_hll_rows(a, h->w, kLearnedLog2p, 1.0, 0u, true, (const uint8_t*)sk, h->w.est, s);
-      launch_mlp_features(row_inputs(h, b), a.rows, feat, s);
+      launch_mlp_features(row_inputs(h->w, b), a.rows, feat, s);
       const cudaError_t e = cudaGetLastError();
       cudaFreeAsync(sk, s);
       OCEAN_CUDA(e);
@@ -1286,7 +1740,7 @@ int ocean_estimate(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_vie
         launch_hll_rows(a, h->w, log2p, 1.0, 0u, true, (const uint8_t*)sk, h->w.est, s);
         MlpModel m = model_of(h);
         if (!with_margin) m.margin = 0.f;
-        launch_mlp_estimate(m, row_inputs(h, b), a.rows, (uint32_t)c.esc_max_products, est, nullptr,
+        launch_mlp_estimate(m, row_inputs(h->w, b), a.rows, (uint32_t)c.esc_max_products, est, nullptr,
                             &h->w.ctr->status, h->num_sms, s);
       } else {
         const double expansion = with_margin ? (log2p == 5 ? 2.0 : 1.5) * c.estimate_scale : 1.0;
@@ -1329,6 +1783,100 @@ int ocean_estimate_metrics(ocean_handle* h, const uint32_t* est, const uint32_t*
     out[1] = m[1] > 0 ? 100.0 * m[2] / m[1] : 0.0;
     out[2] = m[1];
     out[3] = m[3];
+  });
+}
+
+int ocean_batch_create(ocean_handle* h, uint64_t n, const ocean_csr_view* A, const ocean_csr_view* B,
+                       ocean_batch** out, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr && out != nullptr, OCEAN_ERR_INVALID, "handle or out is NULL");
+    *out = nullptr;
+    std::unique_ptr<ocean_batch> b(new ocean_batch());
+    b->h = h;
+    b->cfg = h->cfg;
+    batch_setup(b.get(), n, A, B);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->cfg.batch_autotune && b->rows) batch_autotune(b.get(), s, 5);
+    else batch_plan_and_capture(b.get(), s);
+    *out = b.release();
+  });
+}
+
+int ocean_batch_launch(ocean_batch* b, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(b != nullptr, OCEAN_ERR_INVALID, "batch is NULL");
+    batch_launch(b, (cudaStream_t)stream, false);
+  });
+}
+
+int ocean_batch_run(ocean_batch* b, ocean_csr* C, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(b != nullptr && C != nullptr, OCEAN_ERR_INVALID, "batch or C is NULL");
+    batch_launch(b, (cudaStream_t)stream, true);
+    batch_outputs(b, C);
+  });
+}
+
+int ocean_batch_results(ocean_batch* b, ocean_csr* C) {
+  return guarded([&] {
+    OCEAN_CHECK(b != nullptr && C != nullptr, OCEAN_ERR_INVALID, "batch or C is NULL");
+    batch_outputs(b, C);
+  });
+}
+
+int ocean_batch_info_json(ocean_batch* b, char* buf, size_t cap, size_t* needed) {
+  return guarded([&] {
+    OCEAN_CHECK(b != nullptr, OCEAN_ERR_INVALID, "batch is NULL");
+    std::ostringstream o;
+    o.precision(17);
+    o << "{\"problems\": " << b->n << ", \"rows\": " << b->rows << ", \"nnz_a\": " << b->nnz
+      << ", \"nnz_b\": " << b->bnnz << ", \"nnz_c\": " << b->c_nnz << ", \"workflow\": " << b->wf
+      << ", \"estimator\": \"" << (b->estimator == 2 ? "learned" : b->estimator == 1 ? "hll" : "none")
+      << "\", \"total_est\": " << b->total_est << ", \"kernel_launches\": " << b->launches
+      << ", \"graph\": " << (b->exec ? "true" : "false") << ", \"tuned_ms\": " << b->tuned_ms
+      << ", \"esc_max_products\": " << b->cfg.esc_max_products << ", \"hash_s_max_scale\": "
+      << b->cfg.hash_s_max_scale << ", \"bitmap_words_scale\": " << b->cfg.bitmap_words_scale
+      << ", \"tuning\": \"" << b->tuning << "\"}";
+    const std::string js = o.str();
+    if (needed) *needed = js.size() + 1;
+    OCEAN_CHECK(buf == nullptr || cap >= js.size() + 1, OCEAN_ERR_CAPACITY, "buffer too small");
+    if (buf) std::memcpy(buf, js.c_str(), js.size() + 1);
+  });
+}
+
+int ocean_batch_destroy(ocean_batch* b) {
+  return guarded([&] { delete b; });
+}
+
+int ocean_spgemm_batched(ocean_handle* h, uint64_t n, const ocean_csr_view* A, const ocean_csr_view* B,
+                         ocean_csr* C, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(h != nullptr && C != nullptr, OCEAN_ERR_INVALID, "handle or C is NULL");
+    std::unique_ptr<ocean_batch> b(new ocean_batch());
+    b->h = h;
+    b->cfg = h->cfg;
+    batch_setup(b.get(), n, A, B);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->rows == 0) {
+      b->out_bits = 32;
+      b->c_off.assign(b->n + 1, 0);
+      OCEAN_CUDA(cudaMalloc(&b->c_rp, b->n * 4ull));
+      OCEAN_CUDA(cudaMemset(b->c_rp, 0, b->n * 4ull));
+    } else {
+      batch_run_pipeline(b.get(), s, true);
+    }
+    batch_outputs(b.get(), C);
+    CResult* o = new CResult{0};
+    o->rowptr = b->c_rp;
+    o->col = b->c_col;
+    o->val = b->c_val;
+    o->refs = (int)b->n;
+    o->plain_alloc = true;
+    b->c_rp = nullptr, b->c_col = nullptr, b->c_val = nullptr;  // now owned by the results
+    for (uint32_t p = 0; p < b->n; ++p) {
+      C[p].location = 0;
+      C[p]._owner = o;
+    }
   });
 }
 

@@ -74,7 +74,8 @@ enum DevError : unsigned int {
   DEV_TABLE_FULL = 1u,     // an open-addressing probe exceeded the table size
   DEV_BIN_OVERFLOW = 2u,   // a row did not fit the class it was placed in
   DEV_COUNT_MISMATCH = 4u,  // numeric output count differs from the symbolic count
-  DEV_TC_TIMEOUT = 8u       // a tensor-core completion wait gave up (bounded spin)
+  DEV_TC_TIMEOUT = 8u,      // a tensor-core completion wait gave up (bounded spin)
+  DEV_BATCH_MISMATCH = 16u  // a batch run needed more room than its plan holds; writes were skipped
 };
 
 constexpr uint32_t kUnknownCount = 0xFFFFFFFFu;

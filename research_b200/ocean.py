@@ -35,6 +35,8 @@ EXPORTS = (
     "ocean_murmur3_u32", "ocean_last_error", "ocean_version", "ocean_symbolic_noalloc", "ocean_row_estimates",
     "ocean_mlp_features", "ocean_mlp_forward", "ocean_mlp_grad", "ocean_mlp_adam", "ocean_mlp_builtin",
     "ocean_estimate", "ocean_estimate_metrics",
+    "ocean_batch_create", "ocean_batch_run", "ocean_batch_launch", "ocean_batch_results", "ocean_batch_info_json",
+    "ocean_batch_destroy", "ocean_spgemm_batched",
 )
 
 MLP_FEATURES = 16
@@ -107,6 +109,13 @@ def lib() -> ctypes.CDLL:
     L.ocean_mlp_builtin.argtypes = [vp, ctypes.c_size_t]
     L.ocean_estimate.argtypes = [vp, P(CsrView), P(CsrView), ctypes.c_int, ctypes.c_int, vp, vp]
     L.ocean_estimate_metrics.argtypes = [vp, vp, vp, ctypes.c_uint32, vp, vp]
+    L.ocean_batch_create.argtypes = [vp, u64, P(CsrView), P(CsrView), P(vp), vp]
+    L.ocean_batch_run.argtypes = [vp, P(CsrOut), vp]
+    L.ocean_batch_launch.argtypes = [vp, vp]
+    L.ocean_batch_results.argtypes = [vp, P(CsrOut)]
+    L.ocean_batch_info_json.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, P(ctypes.c_size_t)]
+    L.ocean_batch_destroy.argtypes = [vp]
+    L.ocean_spgemm_batched.argtypes = [vp, u64, P(CsrView), P(CsrView), P(CsrOut), vp]
     L.ocean_last_error.restype = ctypes.c_char_p
     L.ocean_version.restype = ctypes.c_char_p
     for name in EXPORTS:
@@ -327,3 +336,81 @@ def murmur3_device(keys, seed: int = 1234):
     out = torch.empty_like(keys)
     _check(lib().ocean_murmur3_u32(_ptr(keys), _ptr(out), keys.numel(), seed, None))
     return out
+
+
+class Batch:
+    """A batch plan (ocean_batch_*): many independent products run as one
+    captured graph. ``A`` and ``B`` are lists of DeviceCSR (B None: A[p]*A[p]);
+    they must stay alive as long as the plan."""
+
+    def __init__(self, g: "SpGEMM", A, B=None, stream: int = 0):
+        n = len(A)
+        self._g = g
+        self._inputs = (list(A), None if B is None else list(B))
+        self._av = (CsrView * n)(*[a.view() for a in A])
+        self._bv = None if B is None else (CsrView * n)(*[b.view() for b in B])
+        self._h = ctypes.c_void_p()
+        self.n = n
+        _check(lib().ocean_batch_create(g._h, n, self._av, self._bv, ctypes.byref(self._h), stream or None))
+        self._out = (CsrOut * n)()
+
+    def launch(self, stream: int = 0) -> None:
+        _check(lib().ocean_batch_launch(self._h, stream or None))
+
+    def run(self, stream: int = 0) -> list:
+        """One run; returns n DeviceCSR views of the results (valid until the next run)."""
+        _check(lib().ocean_batch_run(self._h, self._out, stream or None))
+        return self._views()
+
+    def results(self) -> list:
+        _check(lib().ocean_batch_results(self._h, self._out))
+        return self._views()
+
+    def _views(self) -> list:
+        views = []
+        for o in self._out:
+            d = DeviceCSR(int(o.rows), int(o.cols), int(o.nnz), None, None, None, int(o.rowptr_bits), _Lent(o))
+            d._plan = self  # the plan owns the memory: keep it alive while a view exists
+            views.append(d)
+        return views
+
+    def info(self) -> dict:
+        need = ctypes.c_size_t(0)
+        _check(lib().ocean_batch_info_json(self._h, None, 0, ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(need.value)
+        _check(lib().ocean_batch_info_json(self._h, buf, need.value, ctypes.byref(need)))
+        return json.loads(buf.value.decode())
+
+    def close(self) -> None:
+        if self._h:
+            lib().ocean_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Lent(CsrOut):
+    """A result view lent by a batch plan (freeing it only clears the struct)."""
+
+    def __init__(self, o: CsrOut):
+        super().__init__()
+        ctypes.memmove(ctypes.addressof(self), ctypes.addressof(o), ctypes.sizeof(CsrOut))
+
+
+def spgemm_batched(g: "SpGEMM", A, B=None, stream: int = 0) -> list:
+    """One-shot batch (ocean_spgemm_batched): owned device results."""
+    n = len(A)
+    av = (CsrView * n)(*[a.view() for a in A])
+    bv = None if B is None else (CsrView * n)(*[b.view() for b in B])
+    out = (CsrOut * n)()
+    _check(lib().ocean_spgemm_batched(g._h, n, av, bv, out, stream or None))
+    res = []
+    for o in out:
+        c = CsrOut()
+        ctypes.memmove(ctypes.addressof(c), ctypes.addressof(o), ctypes.sizeof(CsrOut))
+        res.append(DeviceCSR(int(c.rows), int(c.cols), int(c.nnz), None, None, None, int(c.rowptr_bits), c))
+    return res
