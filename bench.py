@@ -459,6 +459,214 @@ def run_e2e(args, A, B, same, nnz_c, products, world, stream):
             "api": "ocean_spgemm_host (pinned host A/B in, C copied back to pinned host buffers)"}
 
 
+def run_batch(args, world, rank, local):
+    """Workload batch512: 512 independent A_p*A_p (n log-uniform 1k-64k; banded,
+    R-MAT, uniform and block-diagonal in turn; 4-32 entries per row; FP64;
+    generated on the device, seed 5). The learned estimator and the class-policy
+    autotuner are on; one step is one launch of the captured graph of the
+    whole batch. Beside it, the plain form: 512 sequential ocean_spgemm calls
+    per step. e2e: pinned host inputs copied in, the graph, every result copied
+    back (ocean_batch_download); plain e2e: 512 ocean_spgemm_host calls."""
+    import torch
+    from research_b200 import estimator as E
+    from research_b200.ocean import Batch, CsrOut, SpGEMM, _check, lib
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    specs = E.training_specs(512, seed=5, n_lo=1024, n_hi=65536)
+    dA = [E.generate(sp.kind, sp.n, sp.deg, sp.seed, sp.param) for sp in specs]
+    torch.cuda.synchronize()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    # plain: one ocean_spgemm per problem
+    gp = SpGEMM({})
+    products = 0
+    for a in dA:
+        C = gp.multiply(a, a, sptr)
+        products += int(gp.get_stats()["stats"]["intermediate_product"])
+        C.free(sptr)
+    for _ in range(max(0, args.warmup - 1)):
+        for a in dA:
+            gp.multiply(a, a, sptr).free(sptr)
+    e0, e1 = ev(), ev()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        for a in dA:
+            gp.multiply(a, a, sptr).free(sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / args.steps
+
+    # learned + batched: one graph launch per step
+    gb = SpGEMM({"use_learned_estimator": True, "batch_autotune": True})
+    t0 = time.time()
+    plan = Batch(gb, dA, stream=sptr)
+    plan_s = time.time() - t0
+    info = plan.info()
+    for _ in range(args.warmup):
+        plan.launch(sptr)
+    plan.run(sptr)  # checked launch
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = ev(), ev()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.launch(sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    batch_ms = e0.elapsed_time(e1) / args.steps
+    res = plan.run(sptr)
+
+    parity = None
+    if not args.no_check:
+        from oracle import oracle as O
+        worst = 0.0
+        for p in list(range(0, 512, 37)):
+            h = res[p].download()
+            A = dA[p].download()
+            rp, cj, cx, ca = O.spgemm(A, A, with_abs=True)
+            worst = max(worst, O.compare(h.rowptr, h.col, h.val, rp, cj, cx, ca, 1e-12))
+        parity = {"problems_checked": len(range(0, 512, 37)), "max_rel_err": worst, "tolerance": 1e-12}
+
+    # e2e (pinned host copies of every input and of the stacked result)
+    avail = 0
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                avail = int(ln.split()[1]) * 1024
+    except Exception:
+        pass
+    need = 12 * int(info["nnz_c"]) + 24 * int(info["nnz_a"]) + (8 << 30)
+    if avail and avail < need:
+        print(json.dumps({"note": f"e2e skipped: {avail / 2**30:.0f} GiB host memory available, "
+                                  f"{need / 2**30:.0f} GiB needed"}), file=sys.stderr)
+        args.e2e_steps = 0
+
+    def pinned_like(t):
+        return torch.empty(t.shape, dtype=t.dtype, pin_memory=True).copy_(t.cpu())
+    if args.e2e_steps <= 0:
+        raise SystemExit("batch512 needs --e2e-steps >= 1 and enough host memory")
+    hosts = [(pinned_like(a.rowptr), pinned_like(a.col), pinned_like(a.val)) for a in dA]
+    nnz_c = int(info["nnz_c"])
+    rows_tot = int(info["rows"])
+    rp_out = torch.empty(rows_tot + 512, dtype=torch.int64 if info["rowptr_bits"] == 64 else torch.int32,
+                         pin_memory=True)
+    col_out = torch.empty(max(nnz_c, 1), dtype=torch.int32, pin_memory=True)
+    val_out = torch.empty(max(nnz_c, 1), dtype=torch.float64, pin_memory=True)
+    h2d = sum(x.nbytes for hs in hosts for x in hs)
+    d2h = rp_out.nbytes + 12 * nnz_c
+
+    def e2e_step():
+        for a, (r, c, v) in zip(dA, hosts):
+            a.rowptr.copy_(r, non_blocking=True)
+            a.col.copy_(c, non_blocking=True)
+            a.val.copy_(v, non_blocking=True)
+        plan.launch(sptr)
+        plan.download_into(rp_out.numpy(), col_out.numpy(), val_out.numpy(), sptr)
+    e2e_step()
+    e0, e1 = ev(), ev()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+
+    # plain e2e: 512 host-buffer calls
+    from research_b200.ocean import HostCSR
+    hcsr = [HostCSR(a.rows, a.cols, r.numpy().view(np.uint32), c.numpy().view(np.uint32), v.numpy())
+            for a, (r, c, v) in zip(dA, hosts)]
+    out = CsrOut()
+    for m in hcsr:
+        mv = m.view()
+        _check(lib().ocean_spgemm_host(gp._h, ctypes.byref(mv), ctypes.byref(mv), ctypes.byref(out), sptr))
+    e0, e1 = ev(), ev()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        for m in hcsr:
+            mv = m.view()
+            _check(lib().ocean_spgemm_host(gp._h, ctypes.byref(mv), ctypes.byref(mv), ctypes.byref(out), sptr))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+
+    gf = lambda ms: round(2.0 * products / (ms / 1e3) / 1e9, 3)
+    line = {
+        "metric": METRIC + " (batch of 512 independent products)", "value": gf(batch_ms), "unit": "GFLOP/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(batch_ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batch512: 512 x A_p*A_p, n log-uniform 1k-64k, banded/R-MAT/uniform/block-diagonal "
+                               "in turn, 4-32 entries per row, FP64 U[-1,1], seed 5",
+                   "rows": rows_tot, "nnz_A": int(info["nnz_a"]), "nnz_C": nnz_c, "products": products,
+                   "l2": "inputs and outputs (%.1f GB) larger than L2" % ((12 * int(info["nnz_a"]) + 12 * nnz_c) / 1e9)},
+        "plain": {"value": gf(plain_ms), "ms_per_step": round(plain_ms, 3),
+                  "form": "512 sequential ocean_spgemm calls (device inputs)"},
+        "speedup_vs_plain": round(plain_ms / batch_ms, 3),
+        "plan": {"seconds": round(plan_s, 3), **info},
+        "e2e": {"value": gf(e2e_ms), "unit": "GFLOP/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": round(e2e_ms, 3),
+                "api": "pinned host inputs -> device buffers, ocean_batch_launch, ocean_batch_download"},
+        "plain_e2e": {"value": gf(plain_e2e_ms), "ms_per_step": round(plain_e2e_ms, 3),
+                      "api": "512 x ocean_spgemm_host"},
+        "e2e_speedup_vs_plain": round(plain_e2e_ms / e2e_ms, 3),
+        "gpu_launches": int(info["kernel_launches"]) * args.steps,
+        "clocks": clk, "parity": parity,
+    }
+    print(json.dumps(line), flush=True)
+    plan.close()
+
+
+def run_sizing(args, world, rank, local):
+    """Workload rmat21-sizing: the held-out R-MAT (n = 2^21, 24 entries per
+    row, seed 7; generated on the device) whose C (~0.5 TB) is never formed.
+    Times the three ways of sizing every output row: exact symbolic counts
+    (plain precise workflow), HLL estimates (the reference's estimation
+    workflow) and the learned network; and scores the estimates against the
+    exact counts on the rows they size (> 128 products)."""
+    import torch
+    from research_b200 import estimator as E
+    from research_b200.ocean import SpGEMM
+    torch.cuda.set_device(local)
+    A = E.generate("rmat", 1 << 21, 24, seed=7)
+    g = SpGEMM({})
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, out
+
+    exact_ms, truth = timed(lambda: g.symbolic(A, A))
+    res = {}
+    for name in ("learned", "hll"):
+        ms, est = timed(lambda: E.estimate(g, A, None, name, True))
+        m = E.metrics(g, est, truth, 128)
+        m["est_total"] = int((est.to(torch.int64) & 0xFFFFFFFF).sum().item())
+        raw = E.estimate(g, A, None, name, False)
+        mr = E.metrics(g, raw, truth, 128)
+        res[name] = {"ms": round(ms, 3), "prealloc": m, "raw": mr}
+    line = {"workload": "rmat21-sizing: R-MAT n=2^21, 24 entries/row, seed 7; row sizes of C=A*A",
+            "rows": A.rows, "nnz_A": A.nnz, "truth_total": int((truth.to(torch.int64) & 0xFFFFFFFF).sum().item()),
+            "exact_symbolic_ms": round(exact_ms, 3), "learned": res["learned"], "hll": res["hll"],
+            "speedup_learned_vs_exact": round(exact_ms / res["learned"]["ms"], 2),
+            "speedup_learned_vs_hll": round(res["hll"]["ms"] / res["learned"]["ms"], 3),
+            "steps": args.steps, "warmup": args.warmup}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -479,6 +687,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "batch512":
+            run_batch(args, world, rank, local)
+        elif args.workload == "rmat21-sizing":
+            run_sizing(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -215,6 +215,11 @@ int ocean_batch_run(ocean_batch* b, ocean_csr* C, void* stream);
 int ocean_batch_launch(ocean_batch* b, void* stream);
 /* Views of the results of the last completed run (as ocean_batch_run). */
 int ocean_batch_results(ocean_batch* b, ocean_csr* C);
+/* All results of the last completed run into host buffers and wait: rowptrs
+ * receives every problem's row pointers one after another (A[p].rows + 1
+ * values each, of the width in the results' rowptr_bits), col and val the
+ * problems' entries one after another (the sum of their nnz). */
+int ocean_batch_download(ocean_batch* b, void* rowptrs, uint32_t* col, double* val, void* stream);
 /* Plan facts as JSON: sizes, workflow, estimator, kernels per run, tuned policy. */
 int ocean_batch_info_json(ocean_batch* b, char* buf, size_t cap, size_t* needed);
 int ocean_batch_destroy(ocean_batch* b);

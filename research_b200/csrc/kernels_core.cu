@@ -778,7 +778,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     k_sym_bitmap(Csr<RP> A, Csr<RP> B, RowQueue q, DevCounters* __restrict__ ctr,
                  const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
                  const uint32_t* __restrict__ hi, uint32_t* __restrict__ row_nnz, uint64_t* __restrict__ bm_off,
-                 unsigned long long* __restrict__ cache, uint64_t cache_words) {
+                 unsigned long long* __restrict__ cache, uint64_t cache_words, bool unknown_only) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BitmapSymSmem& S = *reinterpret_cast<BitmapSymSmem*>(smem_raw);
   const int tid = threadIdx.x;
@@ -791,6 +791,10 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     const uint32_t idx = S.s_idx;
     if (idx >= count) break;
     const uint32_t row = list[idx];
+    if (unknown_only && row_nnz[row] != kUnknownCount) {  // count already known (uniform over the block)
+      __syncthreads();
+      continue;
+    }
     const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
     const uint64_t rlo = lo[row], rhi = hi[row];
     unsigned long long total = 0;
@@ -1409,7 +1413,8 @@ int launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int nu
   mark(SB_BITMAP);
   if ((gsz = grid(K_SYM_BM, SB_BITMAP, 1)) && ++launched)
     k_sym_bitmap<RP><<<gsz, kBitmapThreads, kSymBitmapSmem, s>>>(A, B, queue(SB_BITMAP), w.ctr, w.prod, w.lo, w.hi,
-                                                                 w.row_nnz, w.bm_off, w.bm_cache, w.bm_cache_words);
+                                                                 w.row_nnz, w.bm_off, w.bm_cache, w.bm_cache_words,
+                                                                 false);
   mark(SB_COUNT);
   return launched;
 }
@@ -1517,7 +1522,7 @@ int launch_overflow(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, bool n
   const RowQueue q{w.ovf, &w.ctr->overflow_n, w.ctr->overflow_cursor + (numeric ? 1 : 0)};
   if (!numeric) {
     k_sym_bitmap<RP><<<num_sms, kBitmapThreads, kSymBitmapSmem, s>>>(A, B, q, w.ctr, w.prod, w.lo, w.hi, w.cnt,
-                                                                     w.bm_off, nullptr, 0);
+                                                                     w.bm_off, nullptr, 0, true);
   } else {
     const OutSpec o{w.rowptr64, w.cnt, nullptr, nullptr, nullptr};
     k_num_bitmap<RP><<<num_sms, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, q, o, w.ctr, w.prod, w.lo, w.hi, w.bm_off,

@@ -120,8 +120,14 @@ __device__ __forceinline__ void row_features(const MlpRowInputs& in, uint64_t ro
   f[5] = log2f(1.f + (float)in.hll[row]);
   f[6] = f[1] - f[0];
   f[7] = f[5] - f[4];
-  f[8] = in.log_b_cols;
-  f[9] = in.log_b_avg;
+  if (in.row_problem) {
+    const float2 c = in.problem_ctx[in.row_problem[row]];
+    f[8] = c.x;
+    f[9] = c.y;
+  } else {
+    f[8] = in.log_b_cols;
+    f[9] = in.log_b_avg;
+  }
   f[10] = f[3] - f[4];
 #pragma unroll
   for (int i = 11; i < kMlpF; ++i) f[i] = 0.f;

@@ -47,6 +47,10 @@ struct MlpRowInputs {
   const uint32_t* hll = nullptr;  // raw HLL union estimate per row
   float log_b_cols = 0.f;         // log2(1 + B.cols)
   float log_b_avg = 0.f;          // log2(1 + nnz(B) / B.rows)
+  // stacked batches: the two B scalars of each row's own problem
+  // (ctx[row_problem[row]] = {log_b_cols, log_b_avg}) instead of the above
+  const uint32_t* row_problem = nullptr;
+  const float2* problem_ctx = nullptr;
 };
 
 // Raw (unnormalised) features of rows [0, n) into feat[n][16].

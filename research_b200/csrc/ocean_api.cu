@@ -1007,6 +1007,8 @@ struct ocean_batch {
   std::vector<uint64_t> a_rows, b_cols;
   BatchProblem* d_probs = nullptr;
   uint64_t* d_pref = nullptr;  // row0 | nnz0 | brow0 | bnnz0 | out0 (n + 1 each)
+  uint32_t* d_row_problem = nullptr;  // problem of every stacked row (learned estimator features)
+  float2* d_ctx = nullptr;            // per problem: log2(1 + B.cols), log2(1 + nnz(B) / B.rows)
   void* a_rp = nullptr;
   uint32_t* a_col = nullptr;
   double* a_val = nullptr;
@@ -1021,7 +1023,7 @@ struct ocean_batch {
   uint8_t* sketch = nullptr;
   unsigned sym_counts[SB_COUNT] = {0};
   unsigned num_counts[NB_COUNT] = {0};
-  uint64_t total_est = 0, c_nnz = 0;
+  uint64_t total_est = 0, c_nnz = 0, products = 0;
   int out_bits = 32;
   uint32_t* t_col = nullptr;
   double* t_val = nullptr;
@@ -1055,7 +1057,7 @@ struct ocean_batch {
     free_arenas();
     free_work_rows(w);
     for (void* p : {(void*)w.ctr, (void*)d_probs, (void*)d_pref, a_rp, (void*)a_col, (void*)a_val, (void*)sketch,
-                    (void*)d_bounds})
+                    (void*)d_bounds, (void*)d_row_problem, (void*)d_ctx})
       if (p) cudaFree(p);
     if (!same_b)
       for (void* p : {b_rp, (void*)b_col, (void*)b_val})
@@ -1115,6 +1117,7 @@ void batch_pipeline(ocean_batch* b, cudaStream_t s, bool plan) {
     batch_readback(b, s);
     const DevCounters& k = *b->h_ctr;
     for (int i = 0; i < SB_COUNT; ++i) b->sym_counts[i] = k.sym_count[i];
+    b->products = k.total_products;
     const Config& c = b->cfg;
     const double avg = A.rows ? (double)k.total_products / (double)A.rows : 0.0;
     if (c.force_workflow == WF_PRECISE) b->wf = WF_PRECISE;
@@ -1147,7 +1150,10 @@ void batch_pipeline(ocean_batch* b, cudaStream_t s, bool plan) {
       launched += launch_hll_sketch_sample(A, B, w, b->log2p, 0u, b->sketch, s);
       if (b->estimator == 2) {
         launched += launch_hll_rows(A, w, b->log2p, 1.0, 0u, true, b->sketch, w.est, s);
-        launched += launch_mlp_estimate(model_of(h), row_inputs(w, B), A.rows, sp.esc_max_products, w.est, nullptr,
+        MlpRowInputs in = row_inputs(w, B);
+        in.row_problem = b->d_row_problem;
+        in.problem_ctx = b->d_ctx;
+        launched += launch_mlp_estimate(model_of(h), in, A.rows, sp.esc_max_products, w.est, nullptr,
                                         &w.ctr->status, h->num_sms, s);
       } else {
         launched += launch_hll_rows(A, w, b->log2p, b->expansion, sp.esc_max_products, false, b->sketch, w.est, s);
@@ -1380,6 +1386,21 @@ void batch_setup(ocean_batch* b, uint64_t n, const ocean_csr_view* A, const ocea
     OCEAN_CUDA(cudaMalloc(&b->b_rp, (b->brows + 1) * rb));
     OCEAN_CUDA(cudaMalloc((void**)&b->b_col, std::max<uint64_t>(b->bnnz, 1) * 4));
     OCEAN_CUDA(cudaMalloc((void**)&b->b_val, std::max<uint64_t>(b->bnnz, 1) * 8));
+  }
+  {
+    // per-row problem ids and per-problem B scalars (the learned estimator's context features)
+    std::vector<uint32_t> rp(std::max<uint64_t>(b->rows, 1));
+    std::vector<float2> ctx(n);
+    for (uint64_t p = 0; p < n; ++p) {
+      for (uint64_t r = b->row0[p]; r < b->row0[p + 1]; ++r) rp[r] = (uint32_t)p;
+      const ocean_csr_view& bb = B ? B[p] : A[p];
+      ctx[p].x = log2f(1.f + (float)bb.cols);
+      ctx[p].y = log2f(1.f + (bb.rows ? (float)((double)bb.nnz / (double)bb.rows) : 0.f));
+    }
+    OCEAN_CUDA(cudaMalloc((void**)&b->d_row_problem, rp.size() * 4));
+    OCEAN_CUDA(cudaMemcpy(b->d_row_problem, rp.data(), rp.size() * 4, cudaMemcpyHostToDevice));
+    OCEAN_CUDA(cudaMalloc((void**)&b->d_ctx, n * sizeof(float2)));
+    OCEAN_CUDA(cudaMemcpy(b->d_ctx, ctx.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
   }
   OCEAN_CUDA(cudaMalloc((void**)&b->w.ctr, sizeof(DevCounters)));
   OCEAN_CUDA(cudaMalloc((void**)&b->d_bounds, (n + 1) * 8));
@@ -1830,7 +1851,9 @@ int ocean_batch_info_json(ocean_batch* b, char* buf, size_t cap, size_t* needed)
     std::ostringstream o;
     o.precision(17);
     o << "{\"problems\": " << b->n << ", \"rows\": " << b->rows << ", \"nnz_a\": " << b->nnz
-      << ", \"nnz_b\": " << b->bnnz << ", \"nnz_c\": " << b->c_nnz << ", \"workflow\": " << b->wf
+      << ", \"nnz_b\": " << b->bnnz << ", \"nnz_c\": " << b->c_nnz << ", \"products\": " << b->products
+      << ", \"rowptr_bits\": " << b->out_bits
+      << ", \"workflow\": " << b->wf
       << ", \"estimator\": \"" << (b->estimator == 2 ? "learned" : b->estimator == 1 ? "hll" : "none")
       << "\", \"total_est\": " << b->total_est << ", \"kernel_launches\": " << b->launches
       << ", \"graph\": " << (b->exec ? "true" : "false") << ", \"tuned_ms\": " << b->tuned_ms
@@ -1841,6 +1864,21 @@ int ocean_batch_info_json(ocean_batch* b, char* buf, size_t cap, size_t* needed)
     if (needed) *needed = js.size() + 1;
     OCEAN_CHECK(buf == nullptr || cap >= js.size() + 1, OCEAN_ERR_CAPACITY, "buffer too small");
     if (buf) std::memcpy(buf, js.c_str(), js.size() + 1);
+  });
+}
+
+int ocean_batch_download(ocean_batch* b, void* rowptrs, uint32_t* col, double* val, void* stream) {
+  return guarded([&] {
+    OCEAN_CHECK(b != nullptr && rowptrs != nullptr, OCEAN_ERR_INVALID, "batch or rowptrs is NULL");
+    OCEAN_CHECK(b->c_nnz == 0 || (col && val), OCEAN_ERR_INVALID, "col or val is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    OCEAN_CUDA(cudaMemcpyAsync(rowptrs, b->c_rp, (b->rows + b->n) * (uint64_t)(b->out_bits / 8),
+                               cudaMemcpyDeviceToHost, s));
+    if (b->c_nnz) {
+      OCEAN_CUDA(cudaMemcpyAsync(col, b->c_col, b->c_nnz * 4, cudaMemcpyDeviceToHost, s));
+      OCEAN_CUDA(cudaMemcpyAsync(val, b->c_val, b->c_nnz * 8, cudaMemcpyDeviceToHost, s));
+    }
+    OCEAN_CUDA(cudaStreamSynchronize(s));
   });
 }
 

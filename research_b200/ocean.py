@@ -36,7 +36,7 @@ EXPORTS = (
     "ocean_mlp_features", "ocean_mlp_forward", "ocean_mlp_grad", "ocean_mlp_adam", "ocean_mlp_builtin",
     "ocean_estimate", "ocean_estimate_metrics",
     "ocean_batch_create", "ocean_batch_run", "ocean_batch_launch", "ocean_batch_results", "ocean_batch_info_json",
-    "ocean_batch_destroy", "ocean_spgemm_batched",
+    "ocean_batch_destroy", "ocean_spgemm_batched", "ocean_batch_download",
 )
 
 MLP_FEATURES = 16
@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
     L.ocean_batch_results.argtypes = [vp, P(CsrOut)]
     L.ocean_batch_info_json.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, P(ctypes.c_size_t)]
     L.ocean_batch_destroy.argtypes = [vp]
+    L.ocean_batch_download.argtypes = [vp, vp, vp, vp, vp]
     L.ocean_spgemm_batched.argtypes = [vp, u64, P(CsrView), P(CsrView), P(CsrOut), vp]
     L.ocean_last_error.restype = ctypes.c_char_p
     L.ocean_version.restype = ctypes.c_char_p
@@ -373,6 +374,10 @@ class Batch:
             d._plan = self  # the plan owns the memory: keep it alive while a view exists
             views.append(d)
         return views
+
+    def download_into(self, rowptrs: np.ndarray, col: np.ndarray, val: np.ndarray, stream: int = 0) -> None:
+        """All results of the last run into (pinned) host arrays, concatenated."""
+        _check(lib().ocean_batch_download(self._h, _ptr(rowptrs), _ptr(col), _ptr(val), stream or None))
 
     def info(self) -> dict:
         need = ctypes.c_size_t(0)
