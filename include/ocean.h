@@ -50,8 +50,9 @@ typedef struct {
 /* Owning CSR result. rowptr has rows+1 entries and rowptr[rows] == nnz (a
  * superset of the reference's contract, which leaves the last offset unspecified).
  * `rowptr_bits` is 32 when nnz < 2^32 (unless the config asks for 64), else 64.
- * `location` is 0 for device memory (free with ocean_csr_free) and 1 for pinned
- * host memory lent by the handle (valid until the next call on that handle). */
+ * `location` is 0 for device memory (free with ocean_csr_free), 1 for pinned
+ * host memory lent by the handle (valid until the next call on that handle) and
+ * 2 for device memory lent by a batch plan (valid until its next run). */
 typedef struct {
   uint64_t rows, cols, nnz;
   void* rowptr;
