@@ -895,82 +895,95 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
         if (one_chunk) block_run_chunk<kBitmapThreads, false>(B, S.e, mark);
         else block_for_each_product<kBitmapThreads, false>(A, B, a0, a1, S.e, mark);
       }
-      // rank table: thread t scans words [16t, 16t+16)
-      const uint32_t wbeg = (uint32_t)tid * kWordsPerThread;
+      // rank table, warp-major so shared-memory reads do not collide: warp w
+      // covers words [512w, 512w + 512), lane l reads words 512w + 32i + l
+      const uint32_t wbase = (uint32_t)warp * 512u;
       uint32_t local = 0;
 #pragma unroll
-      for (int i = 0; i < kWordsPerThread; ++i) {
-        const uint32_t w = wbeg + i;
+      for (int i = 0; i < 16; ++i) {
+        const uint32_t w = wbase + 32u * i + lane;
         local += (w < nwords) ? __popcll(S.bits[w]) : 0u;
       }
+#pragma unroll
+      for (int sh = 16; sh > 0; sh >>= 1) local += __shfl_xor_sync(kFull, local, sh);
       uint32_t nw_total;
-      uint32_t run = block_excl_scan<kBitmapThreads, uint32_t>(local, S.scan, &nw_total);
+      const uint32_t warp_base =
+          __shfl_sync(kFull, block_excl_scan<kBitmapThreads, uint32_t>(lane == 0 ? local : 0u, S.scan, &nw_total), 0);
       if (o.count) {
         // estimation mode (single window): the count is known now; a row that
         // does not fit its slots is listed and skipped
         if (tid == 0) S.s_acc = out_accept(o, ctr, row, nw_total, expect);
         __syncthreads();
         if (!S.s_acc) {
-#pragma unroll
-          for (int i = 0; i < kWordsPerThread; ++i) {
-            const uint32_t w = wbeg + i;
-            if (w < nwords) S.bits[w] = 0ull;
-          }
+          for (uint32_t w = tid; w < nwords; w += kBitmapThreads) S.bits[w] = 0ull;
           __syncthreads();
           off = row_lim;
           break;
         }
       }
-      if ((tid & 63) == 0) S.spre[tid >> 6] = run;
+      // superblock k (words [1024k, 1024k + 1024)) starts with warp 2k
+      if (lane == 0 && (warp & 1) == 0) S.spre[warp >> 1] = warp_base;
       __syncthreads();
-      const uint32_t sp0 = S.spre[tid >> 6];
+      uint32_t run = warp_base - S.spre[warp >> 1];
 #pragma unroll
-      for (int i = 0; i < kWordsPerThread; ++i) {
-        const uint32_t w = wbeg + i;
-        if (w < nwords) {
-          S.wpre[w] = (uint16_t)(run - sp0);
-          run += __popcll(S.bits[w]);
+      for (int i = 0; i < 16; ++i) {
+        const uint32_t w = wbase + 32u * i + lane;
+        const uint32_t pc = (w < nwords) ? (uint32_t)__popcll(S.bits[w]) : 0u;
+        uint32_t x = pc;
+#pragma unroll
+        for (int sh = 1; sh < 32; sh <<= 1) {
+          const uint32_t y = __shfl_up_sync(kFull, x, sh);
+          if (lane >= sh) x += y;
         }
+        if (w < nwords) S.wpre[w] = (uint16_t)(run + x - pc);
+        run += __shfl_sync(kFull, x, 31);
       }
       __syncthreads();
-      // ordered output of the column ids (and zeroed values): 32-word groups go
-      // to the warps round-robin (dense low-index regions spread over all
-      // warps); sparse words are written by one lane each, dense words (more
-      // than 8 bits) by the whole warp with coalesced stores
+      // ordered output of the column ids (and zeroed values): each warp takes
+      // 32-word groups; the group's entries are written in rank order, lane l
+      // writing entries l, l + 32, ... (coalesced): the owner word of an entry
+      // is found by a binary search over the lanes' exclusive counts, its bit
+      // by a 6-step select on the word
       for (uint32_t wb = (uint32_t)warp * 32u; wb < nwords; wb += 32u * (kBitmapThreads / 32)) {
         const uint32_t w = wb + lane;
         const unsigned long long word = w < nwords ? S.bits[w] : 0ull;
-        const uint32_t pre = w < nwords ? S.spre[w >> 10] + S.wpre[w] : 0u;
-        const bool dense = __popcll(word) > 8;
-        if (!dense) {
-          unsigned long long x = word;
-          uint32_t pos = pre;
-          while (x) {
-            const int bpos = __ffsll((long long)x) - 1;
-            x &= x - 1;
-            const uint64_t o = off + pos;
-            if (o < row_lim) {
-              c_col[o] = (uint32_t)(w0 + (uint64_t)w * 64 + bpos);
-              c_val[o] = 0.0;
-            }
-            ++pos;
-          }
-        }
-        unsigned dm = __ballot_sync(kFull, dense);
-        while (dm) {
-          const int src = __ffs(dm) - 1;
-          dm &= dm - 1;
-          const unsigned long long wv = __shfl_sync(kFull, word, src);
-          const uint32_t p0 = __shfl_sync(kFull, pre, src);
+        const uint32_t cnt = (uint32_t)__popcll(word);
+        uint32_t incl = cnt;
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int b = lane + 32 * h;
-            if ((wv >> b) & 1ull) {
-              const uint64_t o = off + p0 + __popcll(wv & ((1ull << b) - 1ull));
-              if (o < row_lim) {
-                c_col[o] = (uint32_t)(w0 + (uint64_t)(wb + src) * 64 + b);
-                c_val[o] = 0.0;
+        for (int sh = 1; sh < 32; sh <<= 1) {
+          const uint32_t y = __shfl_up_sync(kFull, incl, sh);
+          if (lane >= sh) incl += y;
+        }
+        const uint32_t excl = incl - cnt;
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        if (total == 0) continue;
+        const uint32_t gpre = S.spre[wb >> 10] + S.wpre[wb];
+        const uint32_t rounds = (total + 31) >> 5;
+        for (uint32_t rd = 0; rd < rounds; ++rd) {
+          const uint32_t j = rd * 32 + lane;
+          uint32_t k = 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const uint32_t e = __shfl_sync(kFull, excl, k + step);
+            if (e <= j) k += step;
+          }
+          unsigned long long x = __shfl_sync(kFull, word, k);
+          uint32_t r = j - __shfl_sync(kFull, excl, k);
+          if (j < total) {
+            uint32_t pos = 0;
+#pragma unroll
+            for (int sb = 32; sb > 0; sb >>= 1) {
+              const uint32_t c = (uint32_t)__popcll(x & ((1ull << sb) - 1ull));
+              if (r >= c) {
+                r -= c;
+                x >>= sb;
+                pos += sb;
               }
+            }
+            const uint64_t o = off + gpre + j;
+            if (o < row_lim) {
+              c_col[o] = (uint32_t)(w0 + (uint64_t)(wb + k) * 64 + pos);
+              c_val[o] = 0.0;
             }
           }
         }
@@ -987,11 +1000,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       };
       if (one_chunk) block_run_chunk<kBitmapThreads, true>(B, S.e, accumulate);
       else block_for_each_product<kBitmapThreads, true>(A, B, a0, a1, S.e, accumulate);
-#pragma unroll
-      for (int i = 0; i < kWordsPerThread; ++i) {
-        const uint32_t w = wbeg + i;
-        if (w < nwords) S.bits[w] = 0ull;
-      }
+      for (uint32_t w = tid; w < nwords; w += kBitmapThreads) S.bits[w] = 0ull;
       off += nw_total;
       __syncthreads();
     }
