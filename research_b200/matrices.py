@@ -10,6 +10,10 @@ distributions of the benchmark configurations:
 * :func:`banded`, :func:`uniform_random`, :func:`block_diagonal` — the mixed
   families of the learned-estimator and batched workloads.
 
+:func:`read_mtx` reads MatrixMarket coordinate files like the reference's
+converter (utils/convert.cpp:83-240), so real matrices can be used where they
+are available.
+
 ``.hicsr`` layout (reference src/CSR.cpp:70-152): an 80-byte header (9-byte
 magic ``'H','i',1,'C','o','m','p','s','d'`` padded to 16, then eight uint64:
 typesize, compresseddir, indexsize, fixedoffset, offsetsize, rows, cols, nnz),
@@ -187,3 +191,66 @@ def read_hicsr(path) -> HostCSR:
     off += nnz * 4
     rowptr = np.frombuffer(data, np.uint32, rows + 1, off).copy()
     return HostCSR(int(rows), int(cols), rowptr, col, val)
+
+
+def read_mtx(path) -> HostCSR:
+    """Reads a MatrixMarket coordinate file the way the reference's converter
+    does (utils/convert.cpp:83-240): header ``%%MatrixMarket matrix coordinate
+    <type> <symmetry>``; type real, integer or double (values read as FP64),
+    pattern (every value 1.0) or complex (the real part); symmetry general,
+    symmetric or Hermitian, where every off-diagonal entry (r, c) is mirrored
+    to (c, r) with the same value; 1-based indices checked against the size
+    line; entries sorted by (row, column) with duplicates kept (in file order,
+    where the reference's sort leaves their order open). Raises ValueError."""
+    import io
+    text = Path(path).read_text()
+    lines = text.splitlines()
+    if not lines or not lines[0].startswith("%%MatrixMarket matrix coordinate"):
+        raise ValueError("Can only read MatrixMarket format that is in coordinate form")
+    tok = lines[0].split()
+    if len(tok) < 5:
+        raise ValueError("incomplete MatrixMarket header")
+    kind, sym = tok[3], tok[4]
+    if kind not in ("pattern", "complex", "real", "integer", "double"):
+        raise ValueError("MatrixMarket data type does not match matrix format")
+    if sym not in ("general", "symmetric", "Hermitian"):
+        raise ValueError("Can only read MatrixMarket format that is either symmetric, general or hermitian")
+    i = 1
+    while i < len(lines) and (not lines[i].strip() or lines[i].lstrip().startswith("%")):
+        i += 1
+    if i >= len(lines):
+        raise ValueError("Failed to read matrix market header")
+    size = lines[i].split()
+    try:
+        rows, cols, nnz = int(size[0]), int(size[1]), int(size[2])
+    except (IndexError, ValueError):
+        raise ValueError("Failed to read matrix market header")
+    body = [ln for ln in lines[i + 1:] if ln.strip() and not ln.lstrip().startswith("%")]
+    ncol = 2 if kind == "pattern" else 3
+    if body:
+        try:
+            arr = np.loadtxt(io.StringIO("\n".join(body)), ndmin=2, usecols=range(ncol), dtype=np.float64)
+        except ValueError as e:
+            raise ValueError(f"Failed to read data from matrix market file: {e}")
+    else:
+        arr = np.zeros((0, ncol))
+    r = arr[:, 0].astype(np.int64)
+    c = arr[:, 1].astype(np.int64)
+    v = np.ones(r.size) if kind == "pattern" else arr[:, 2].astype(np.float64)
+    if r.size and (r.min() < 1 or r.max() > rows):
+        raise ValueError("Row index out of bounds in matrix market file")
+    if c.size and (c.min() < 1 or c.max() > cols):
+        raise ValueError("Column index out of bounds in matrix market file")
+    r, c = r - 1, c - 1
+    if sym != "general":
+        off = r != c
+        # mirrored entry right after its original, as the reference appends it
+        order = np.argsort(np.concatenate([np.arange(r.size) * 2, np.nonzero(off)[0] * 2 + 1]), kind="stable")
+        r = np.concatenate([r, c[off]])[order]
+        c2 = np.concatenate([c, arr[:, 0].astype(np.int64)[off] - 1])[order]
+        v = np.concatenate([v, v[off]])[order]
+        c = c2
+    key = r * max(cols, 1) + c
+    order = np.argsort(key, kind="stable")
+    return _from_coo_sorted(rows, cols, r[order], c[order], v[order])
+
