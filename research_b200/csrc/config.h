@@ -180,6 +180,7 @@ struct Config {
   int hll_sample_min_rows = 648;
   int hll_sample_max_rows = 10800;
   int hll_higher_precision_expansion_threshold = 48;
+  int fat_ratio = 100;
   // this library's keys
   int output_rowptr_bits = 0;     // 0: 32 when nnz(C) < 2^32, else 64
   int esc_max_products = 128;     // rows with at most this many products use the register ESC classes
@@ -189,7 +190,7 @@ struct Config {
   double bitmap_cache_fraction = 0.25;  // share of free device memory the saved row bitmaps may use
   int small_problem_nnz = 1 << 20;      // A with at most this many entries: no read-back after analysis
   int spin_wait_us = 2000;              // poll the stream this long before a blocking synchronize
-  int force_workflow = -1;              // -1 auto; 0 precise, 1 estimation (HLL), 2 ultra-sparse
+  int force_workflow = -1;              // -1 auto; 0 precise, 1 estimation (HLL), 2 ultra-sparse, 3 fat
   double estimate_scale = 1.0;          // multiplies the HLL expansion (testing: < 1 forces overflows)
   bool use_learned_estimator = false;   // estimation workflow: per-row sizes from the MLP instead of HLL
   std::string learned_estimator_weights;  // weights file; empty: the built-in trained network
@@ -262,6 +263,7 @@ struct Config {
     geti("small_problem_nnz", c.small_problem_nnz);
     geti("spin_wait_us", c.spin_wait_us);
     geti("force_workflow", c.force_workflow);
+    geti("fat_ratio", c.fat_ratio);
     getd("estimate_scale", c.estimate_scale);
     getb("use_learned_estimator", c.use_learned_estimator);
     gets("learned_estimator_weights", c.learned_estimator_weights);
@@ -272,8 +274,8 @@ struct Config {
     getb("batch_autotune", c.batch_autotune);
     if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
-    if (c.force_workflow < -1 || c.force_workflow > 2)
-      throw std::invalid_argument("force_workflow must be -1, 0, 1 or 2");
+    if (c.force_workflow < -1 || c.force_workflow > 3)
+      throw std::invalid_argument("force_workflow must be -1, 0, 1, 2 or 3");
     if (c.estimate_scale <= 0.0) throw std::invalid_argument("estimate_scale must be positive");
     if (c.bitmap_cache_fraction < 0.0 || c.bitmap_cache_fraction > 0.9)
       throw std::invalid_argument("bitmap_cache_fraction must be in [0, 0.9]");

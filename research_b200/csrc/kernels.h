@@ -127,6 +127,9 @@ int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const O
 
 void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, cudaStream_t s);
 
+// out[r] = min(products, column span) for every row of the last analysis.
+int launch_row_bounds(const DevWork& w, uint32_t* out, cudaStream_t s);
+
 // Per-kernel dynamic shared memory opt-in; call once per device.
 void configure_kernel_attributes();
 

@@ -1300,6 +1300,18 @@ __global__ void __launch_bounds__(256) k_copy_rows(uint64_t rows, const uint64_t
   }
 }
 
+// out[r] = min(products, column span) of row r: an exact upper bound of its
+// output count (0 for rows without products).
+__global__ void __launch_bounds__(256) k_row_bounds(uint64_t rows, const uint32_t* __restrict__ prod,
+                                                    const uint32_t* __restrict__ lo,
+                                                    const uint32_t* __restrict__ hi, uint32_t* __restrict__ out) {
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = prod[r];
+    const uint64_t span = p ? (uint64_t)hi[r] - lo[r] + 1 : 0;
+    out[r] = (uint32_t)(p < span ? p : span);
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 namespace {
 constexpr size_t kNumBitmapSmem = sizeof(BitmapNumSmem);
@@ -1481,6 +1493,13 @@ int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const O
                                                                  w.hi, w.bm_off, w.bm_cache, c_col, c_val);
   mark(NB_COUNT);
   return launched;
+}
+
+int launch_row_bounds(const DevWork& w, uint32_t* out, cudaStream_t s) {
+  if (w.rows == 0) return 0;
+  const uint64_t blocks = std::min<uint64_t>((w.rows + 255) / 256, 148ull * 16);
+  k_row_bounds<<<(unsigned)blocks, 256, 0, s>>>(w.rows, w.prod, w.lo, w.hi, out);
+  return 1;
 }
 
 void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, cudaStream_t s) {

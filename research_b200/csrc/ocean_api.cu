@@ -524,7 +524,10 @@ MlpRowInputs row_inputs(const DevWork& w, const Csr<RP>& B) {
 constexpr int kLearnedLog2p = 5;
 
 // Workflow ids as reported in the stats (reference: kernels/SpGEMM.cuh:1807-1817).
-enum Workflow { WF_PRECISE = 0, WF_ESTIMATION = 1, WF_ULTRASPARSE = 2 };
+// Output columns below which the FAT workflow applies: the reference's largest
+// dense numeric bin, 64 KB / 9 B - 4 (include/Common.h:78-110,261-269).
+constexpr uint64_t kFatMaxCols = 7277;
+enum Workflow { WF_PRECISE = 0, WF_ESTIMATION = 1, WF_ULTRASPARSE = 2, WF_FAT = 3 };
 
 // Chooses the workflow after the analysis (reference rules,
 // kernels/SpGEMM.cuh:456-540 and kernels/Analysis.cuh:10-29):
@@ -539,6 +542,16 @@ enum Workflow { WF_PRECISE = 0, WF_ESTIMATION = 1, WF_ULTRASPARSE = 2 };
 template <typename RP>
 int choose_workflow(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool readback) {
   const Config& c = h->cfg;
+  // short, fat A times tall, skinny B with few output columns
+  // (kernels/SpGEMM.cuh:456-466): every row gets its exact upper bound
+  // min(products, span) <= B.cols as its slots, so nothing overflows
+  const bool fat = c.use_fat_workflow && c.fat_ratio > 0 && A.cols / (uint64_t)c.fat_ratio > A.rows &&
+                   B.rows / (uint64_t)c.fat_ratio > B.cols && B.cols < kFatMaxCols;
+  if (c.force_workflow == WF_FAT || (c.force_workflow < 0 && fat)) {
+    h->st.launches += launch_row_bounds(h->w, h->w.est, s);
+    h->st.estimator = 3;
+    return WF_FAT;
+  }
   if (c.force_workflow == WF_PRECISE || (!readback && c.force_workflow < 0)) return WF_PRECISE;
   const DevCounters& k = *h->h_ctr;
   const uint64_t products = readback ? k.total_products : 0;
@@ -691,7 +704,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         h->seg_ran = true;
       }
       wf = choose_workflow(h, A, B, s, readback);
-      if (wf == WF_ESTIMATION || wf == WF_ULTRASPARSE) {
+      if (wf == WF_ESTIMATION || wf == WF_ULTRASPARSE || wf == WF_FAT) {
         // scan of the estimates: temporary slots per row, numeric classes by estimate
         st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s);
         OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
@@ -874,10 +887,11 @@ std::string stats_json(ocean_handle* h) {
   if (st.sampled)
     o << "\"sampling\": {\"compaction_1\": " << st.compaction1 << ", \"compaction_2\": " << st.compaction2
       << "}, ";
-  if (st.workflow == 1 || st.workflow == 2) {
+  if (st.workflow == 1 || st.workflow == 2 || st.workflow == 3) {
     o << "\"estimation\": {\"overflow_rows\": " << st.overflow_rows << ", \"log2_precision\": " << st.hll_log2p
       << ", \"total_est\": " << st.total_est << ", \"expansion\": " << st.hll_expansion << ", \"estimator\": \""
-      << (st.estimator == 2 ? "learned" : st.estimator == 1 ? "hll" : "products") << "\"";
+      << (st.estimator == 3 ? "bound" : st.estimator == 2 ? "learned" : st.estimator == 1 ? "hll" : "products")
+      << "\"";
     if (st.metrics)
       o << ", \"metrics\": {\"rows\": " << st.metric_rows << ", \"mean_rel_error\": " << st.mre
         << ", \"misbinned_pct\": " << st.misbinned << ", \"mean_rel_error_raw\": " << st.mre_raw
