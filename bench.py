@@ -151,6 +151,105 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+class NvmlSampler:
+    """In-process NVML sampling of SM clocks, power and clock-event reasons
+    during the timed region (a thread, one query set every 200 ms). Spawning
+    nvidia-smi instead stalls the host's CUDA calls at each of its samples,
+    which shows in multiplies of a millisecond or less."""
+    PERIOD_S = 0.2
+
+    def __init__(self, device: int):
+        import threading
+        self.device = device
+        self.rows = []
+        self.error = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._nv = None
+        self._h = None
+
+    def _handle(self):
+        import pynvml as nv
+        import torch
+        p = torch.cuda.get_device_properties(self.device)
+        for get in (lambda: nv.nvmlDeviceGetHandleByPciBusId(
+                        f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"),
+                    lambda: nv.nvmlDeviceGetHandleByUUID("GPU-" + str(p.uuid)),
+                    lambda: nv.nvmlDeviceGetHandleByIndex(self.device)):
+            try:
+                return get()
+            except Exception:
+                continue
+        raise RuntimeError("no NVML handle for the device")
+
+    def _sample(self):
+        nv, h = self._nv, self._h
+        reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                          nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                          nv.nvmlDeviceGetPowerUsage(h) / 1000.0, reasons))
+
+    def _loop(self):
+        while not self._stop.wait(self.PERIOD_S):
+            try:
+                self._sample()
+            except Exception as e:  # keep the timing; report the sampler's failure
+                self.error = str(e)
+                return
+
+    def start(self) -> bool:
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self._nv = nv
+            self._h = self._handle()
+            self._sample()  # one sample before the timed region
+        except Exception as e:
+            self.error = str(e)
+            return False
+        self._thread = threading.Thread(target=self._loop, daemon=True)
+        self._thread.start()
+        return True
+
+    def stop(self) -> dict:
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+            try:
+                self._sample()  # and one at its end
+            except Exception as e:
+                self.error = self.error or str(e)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"no samples ({self.error})"]}
+        nv = self._nv
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap,
+                "hw_power_brake_slowdown": nv.nvmlClocksEventReasonHwPowerBrakeSlowdown}
+        reasons = sorted({k for r in self.rows for k, b in bits.items() if r[3] & b})
+        sm = [float(r[0]) for r in self.rows]
+        mx = max(float(r[1]) for r in self.rows)
+        load = [x for x in sm if x > 0.5 * mx] or sm
+        out = {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": reasons,
+               "samples": len(self.rows), "power_w_max": round(max(r[2] for r in self.rows), 1),
+               "source": "nvml"}
+        if self.error:
+            out["sampler_error"] = self.error
+        return out
+
+
+def clock_sampler(device: int):
+    """NVML in-process sampler; nvidia-smi when NVML is not importable."""
+    s = NvmlSampler(device)
+    try:
+        import pynvml  # noqa: F401
+        return s
+    except ImportError:
+        return ClockSampler(device)
+
+
 # ----------------------------------------------------------------------------- CPU leg
 def take_rows(A, rows: np.ndarray):
     from research_b200.ocean import HostCSR
@@ -310,7 +409,7 @@ def run_ours(args, world, rank, local):
     st0 = g0.get_stats()
     nnz_c = int(st0["C"]["nnz"])
     products = int(st0["stats"]["intermediate_product"])
-    clocks = ClockSampler(local)
+    clocks = clock_sampler(local)
     torch.cuda.synchronize()
     barrier(world)
     clocks.start()
@@ -530,7 +629,7 @@ def run_batch(args, world, rank, local):
     for _ in range(args.warmup):
         plan.launch(sptr)
     plan.run(sptr)  # checked launch
-    clocks = ClockSampler(local)
+    clocks = clock_sampler(local)
     clocks.start()
     e0, e1 = ev(), ev()
     torch.cuda.synchronize()
