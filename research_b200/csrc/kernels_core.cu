@@ -592,8 +592,8 @@ struct SymHashSmem {
 
 template <typename RP, int NT, int LOG2T>
 __global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, RowQueue q, DevCounters* __restrict__ ctr,
-                                                 const uint32_t* __restrict__ prod,
-                                                 uint32_t* __restrict__ row_nnz) {
+                                                 const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
+                                                 const uint32_t* __restrict__ hi, uint32_t* __restrict__ row_nnz) {
   constexpr int T = 1 << LOG2T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SymHashSmem<NT, LOG2T>& S = *reinterpret_cast<SymHashSmem<NT, LOG2T>*>(smem_raw);
@@ -607,11 +607,14 @@ __global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, RowQueue 
     const uint32_t idx = S.s_idx;
     if (idx >= count) break;
     const uint32_t row = list[idx];
+    // a row whose column span fits the table addresses it directly: slot = column - lo
+    const uint32_t rlo = lo[row];
+    const bool direct = hi[row] - rlo < (uint32_t)T;
     unsigned cnt = 0;
     bool full = false;
     block_for_each_product<NT, false>(A, B, A.row_begin(row), A.row_end(row), S.e, [&](uint32_t c, double, bool ok) {
       if (!ok) return;
-      uint32_t h = hash_slot(c, LOG2T);
+      uint32_t h = direct ? c - rlo : hash_slot(c, LOG2T);
       int probe = 0;
       for (; probe < T; ++probe) {
         const uint32_t cur = S.keys[h];
@@ -649,6 +652,7 @@ struct NumHashSmem {
 template <typename RP, int NT, int LOG2T>
 __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, RowQueue q, OutSpec o,
                                                  DevCounters* __restrict__ ctr, const uint32_t* __restrict__ prod,
+                                                 const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
                                                  uint32_t* __restrict__ c_col, double* __restrict__ c_val) {
   constexpr int T = 1 << LOG2T;
   constexpr int PER = T / NT;
@@ -672,10 +676,14 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, RowQueue 
     const uint32_t idx = S.s_idx;
     if (idx >= count) break;
     const uint32_t row = list[idx];
+    // a row whose column span fits the table addresses it directly (slot =
+    // column - lo): no probing, and the slots are already in column order
+    const uint32_t rlo = lo[row];
+    const bool direct = hi[row] - rlo < (uint32_t)T;
     bool full = false;
     block_for_each_product<NT, true>(A, B, A.row_begin(row), A.row_end(row), S.e, [&](uint32_t c, double v, bool ok) {
       if (!ok) return;
-      uint32_t h = hash_slot(c, LOG2T);
+      uint32_t h = direct ? c - rlo : hash_slot(c, LOG2T);
       int probe = 0;
       for (; probe < T; ++probe) {
         const uint32_t cur = S.keys[h];
@@ -698,6 +706,38 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, RowQueue 
     // with unknown count in estimation mode
     const int any_full = __syncthreads_or(full);
     if (any_full && tid == 0 && !o.count) raise_status(ctr, DEV_TABLE_FULL, row);
+    if (direct) {
+      // ordered compaction: thread t owns slots [t * PER, t * PER + PER); a
+      // block scan of the occupied counts gives each thread its output position
+      unsigned cnt = 0;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) cnt += S.keys[tid * PER + i] != kEmpty;
+      unsigned long long n64;
+      const unsigned long long pos0 = block_excl_scan<NT, unsigned long long>(cnt, S.e.scan, &n64);
+      const uint32_t n = (uint32_t)n64;
+      const uint32_t cap = o.cap[row];
+      if (tid == 0) S.s_acc = out_accept(o, ctr, row, n, cap);
+      __syncthreads();
+      const uint32_t wn = S.s_acc ? min(n, cap) : 0u;
+      const uint64_t off = o.off[row];
+      uint32_t w = (uint32_t)pos0;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const uint32_t sl = tid * PER + i;
+        const uint32_t key = S.keys[sl];
+        if (key != kEmpty) {
+          if (w < wn) {
+            c_col[off + w] = key;
+            c_val[off + w] = S.vals[sl];
+          }
+          ++w;
+          S.keys[sl] = kEmpty;
+          S.vals[sl] = 0.0;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     // compaction: read this thread's slots, then rewrite the key area as sort keys
     uint32_t mine[PER];
     unsigned cnt = 0;
@@ -1422,15 +1462,15 @@ int launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int nu
   mark(SB_HASH_S);
   if ((gsz = grid(K_SYM_S, SB_HASH_S, 1)) && ++launched)
     k_sym_hash<RP, 128, 11><<<gsz, 128, sym_hash_smem<128, 11>(), s>>>(A, B, queue(SB_HASH_S), w.ctr, w.prod,
-                                                                       w.row_nnz);
+                                                                       w.lo, w.hi, w.row_nnz);
   mark(SB_HASH_M);
   if ((gsz = grid(K_SYM_M, SB_HASH_M, 1)) && ++launched)
     k_sym_hash<RP, 256, 13><<<gsz, 256, sym_hash_smem<256, 13>(), s>>>(A, B, queue(SB_HASH_M), w.ctr, w.prod,
-                                                                       w.row_nnz);
+                                                                       w.lo, w.hi, w.row_nnz);
   mark(SB_HASH_L);
   if ((gsz = grid(K_SYM_L, SB_HASH_L, 1)) && ++launched)
     k_sym_hash<RP, 512, 15><<<gsz, 512, sym_hash_smem<512, 15>(), s>>>(A, B, queue(SB_HASH_L), w.ctr, w.prod,
-                                                                       w.row_nnz);
+                                                                       w.lo, w.hi, w.row_nnz);
   mark(SB_BITMAP);
   if ((gsz = grid(K_SYM_BM, SB_BITMAP, 1)) && ++launched)
     k_sym_bitmap<RP><<<gsz, kBitmapThreads, kSymBitmapSmem, s>>>(A, B, queue(SB_BITMAP), w.ctr, w.prod, w.lo, w.hi,
@@ -1478,15 +1518,15 @@ int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const O
   mark(NB_HASH_S);
   if ((gsz = grid(K_NUM_S, NB_HASH_S, 1)) && ++launched)
     k_num_hash<RP, 128, 10><<<gsz, 128, num_hash_smem<128, 10>(), s>>>(A, B, queue(NB_HASH_S), o, w.ctr, w.prod,
-                                                                       c_col, c_val);
+                                                                       w.lo, w.hi, c_col, c_val);
   mark(NB_HASH_M);
   if ((gsz = grid(K_NUM_M, NB_HASH_M, 1)) && ++launched)
     k_num_hash<RP, 256, 12><<<gsz, 256, num_hash_smem<256, 12>(), s>>>(A, B, queue(NB_HASH_M), o, w.ctr, w.prod,
-                                                                       c_col, c_val);
+                                                                       w.lo, w.hi, c_col, c_val);
   mark(NB_HASH_L);
   if ((gsz = grid(K_NUM_L, NB_HASH_L, 1)) && ++launched)
     k_num_hash<RP, 512, 13><<<gsz, 512, num_hash_smem<512, 13>(), s>>>(A, B, queue(NB_HASH_L), o, w.ctr, w.prod,
-                                                                       c_col, c_val);
+                                                                       w.lo, w.hi, c_col, c_val);
   mark(NB_BITMAP);
   if ((gsz = grid(K_NUM_BM, NB_BITMAP, 1)) && ++launched)
     k_num_bitmap<RP><<<gsz, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, queue(NB_BITMAP), o, w.ctr, w.prod, w.lo,

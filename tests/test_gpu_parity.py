@@ -178,7 +178,8 @@ def test_errors_are_status_codes():
         SpGEMM({"use_hybrid_accumulator": True, "use_indirect_sort": False}).multiply(A, A)
     assert e.value.code == 4
     # a row forced into a class too small for it is reported, not mis-written
-    R = M.block_diagonal(4096, 1024, 64, seed=2)
+    # (2048-column blocks: wider than the 1024 slots, so the rows are hashed)
+    R = M.block_diagonal(8192, 2048, 64, seed=2)
     with pytest.raises(OceanError) as e:
         multiply_device(R, R, {"force_num_bin": NUM_BINS["hash_s"]})
     assert e.value.code in (2, 6)
