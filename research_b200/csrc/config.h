@@ -198,6 +198,7 @@ struct Config {
   bool estimator_metrics = false;       // after an estimated multiply: error of the estimates vs exact counts
   double hash_s_max_scale = 1.0;        // (0, 1]: fill limit of the small hash tables relative to the default
   double bitmap_words_scale = 1.0;      // > 0: scales the column-span limits under which mid rows use bitmaps
+  bool prefer_direct_hash = true;       // mid rows whose column span fits a hash table use it (direct slots)
   bool batch_autotune = false;          // batched plans: search the class policy on the batch before capturing
 
   static Config from_json_text(const std::string& text) {
@@ -271,6 +272,7 @@ struct Config {
     getb("estimator_metrics", c.estimator_metrics);
     getd("hash_s_max_scale", c.hash_s_max_scale);
     getd("bitmap_words_scale", c.bitmap_words_scale);
+    getb("prefer_direct_hash", c.prefer_direct_hash);
     getb("batch_autotune", c.batch_autotune);
     if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");

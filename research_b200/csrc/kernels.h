@@ -42,6 +42,7 @@ struct SymPolicy {
   uint32_t hash_s_max = 1024;       // products of a small-hash row (table of 2048 slots)
   uint32_t bm_words_m = 2048;       // 4096-product rows: bitmap when the span needs at most this many words
   uint32_t bm_words_l = 8192;       // larger rows up to 16384 products: same rule
+  uint32_t direct = 1;              // mid rows whose span fits a hash table take it (direct slots), not a bitmap
 };
 struct NumPolicy {
   uint32_t esc_max_products = 128;
@@ -49,6 +50,7 @@ struct NumPolicy {
   uint32_t hash_s_max = 512;        // outputs of a small-hash row (table of 1024 slots)
   uint32_t bm_words_m = 1024;
   uint32_t bm_words_l = 4096;
+  uint32_t direct = 1;
 };
 
 // Symbolic class of a row from its product count and output column span.
@@ -58,8 +60,8 @@ __device__ __forceinline__ int sym_bin_for(uint64_t p, uint64_t span, const SymP
   const uint64_t words = (span + 63) >> 6;
   if (p > 16384) return SB_BITMAP;
   if (p <= pol.hash_s_max) return SB_HASH_S;
-  if (p <= 4096) return (words <= pol.bm_words_m) ? SB_BITMAP : SB_HASH_M;
-  return (words <= pol.bm_words_l) ? SB_BITMAP : SB_HASH_L;
+  if (p <= 4096) return ((pol.direct && span <= 8192) || words > pol.bm_words_m) ? SB_HASH_M : SB_BITMAP;
+  return ((pol.direct && span <= 32768) || words > pol.bm_words_l) ? SB_HASH_L : SB_BITMAP;
 }
 
 // Numeric class of a row from its exact output count.
@@ -70,8 +72,8 @@ __device__ __forceinline__ int num_bin_for(uint32_t n, uint64_t p, uint64_t span
   if (p <= pol.esc_max_products) return p <= 32 ? NB_ESC1 : (p <= 64 ? NB_ESC2 : NB_ESC4);
   const uint64_t words = (span + 63) >> 6;
   if (n <= pol.hash_s_max) return NB_HASH_S;
-  if (n <= 2048) return (words <= pol.bm_words_m) ? NB_BITMAP : NB_HASH_M;
-  if (n <= 4096) return (words <= pol.bm_words_l) ? NB_BITMAP : NB_HASH_L;
+  if (n <= 2048) return ((pol.direct && span <= 4096) || words > pol.bm_words_m) ? NB_HASH_M : NB_BITMAP;
+  if (n <= 4096) return ((pol.direct && span <= 8192) || words > pol.bm_words_l) ? NB_HASH_L : NB_BITMAP;
   return NB_BITMAP;
 }
 

@@ -98,6 +98,9 @@ struct Stats {
   int rowptr_bits = 32;
   bool valid = false;
   double host_ms = 0.0;
+  // host clock at the steps of the last multiply (ms since its start): where a
+  // call that is short on the device spends its time between read-backs
+  std::vector<std::pair<const char*, double>> host_marks;
   // estimation workflows: which estimator sized the rows, and (estimator_metrics)
   // its error against the exact counts: mean relative row-size error and share
   // of rows whose numeric class differs, with and without the safety margin
@@ -365,6 +368,7 @@ void make_policies(const Config& c, SymPolicy* sp, NumPolicy* np) {
   sp->bm_words_l = (uint32_t)(sp->bm_words_l * c.bitmap_words_scale);
   np->bm_words_m = (uint32_t)(np->bm_words_m * c.bitmap_words_scale);
   np->bm_words_l = (uint32_t)(np->bm_words_l * c.bitmap_words_scale);
+  sp->direct = np->direct = c.prefer_direct_hash ? 1u : 0u;
   OCEAN_CHECK(sp->force_bin < SB_COUNT && np->force_bin < NB_COUNT, OCEAN_ERR_INVALID, "forced class out of range");
 }
 
@@ -675,6 +679,9 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   const Csr<RP> B = to_csr<RP>(Bv, brp);
   Stats& st = h->st;
   st = Stats();
+  auto mark = [&](const char* what) {
+    st.host_marks.emplace_back(what, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  };
   st.a_rows = A.rows, st.a_cols = A.cols, st.a_nnz = A.nnz;
   st.b_rows = B.rows, st.b_cols = B.cols, st.b_nnz = B.nnz;
   h->ev_recorded = false;
@@ -695,6 +702,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   try {
     if (A.rows > 0) {
       const bool readback = run_analysis(h, A, B, s);
+      mark("analysis");
       if (h->cfg.use_segmented_workflow) {
         // analysis-only pass: its records go to the stats (reference: kernels/SpGEMM.cuh:240-259)
         const Config& c = h->cfg;
@@ -704,7 +712,17 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         h->seg_ran = true;
       }
       wf = choose_workflow(h, A, B, s, readback);
-      if (wf == WF_ESTIMATION || wf == WF_ULTRASPARSE || wf == WF_FAT) {
+      mark("workflow");
+      // numeric class sizes on the host (grids capped by class size); without
+      // them every class is launched at full grid
+      bool class_counts = true;
+      if (wf == WF_ULTRASPARSE && readback) {
+        // the estimates are the product counts, whose total the analysis read
+        // back and choose_workflow checked against free memory: no read-back
+        st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s);
+        st.total_est = h->h_ctr->total_products;
+        class_counts = false;
+      } else if (wf == WF_ESTIMATION || wf == WF_ULTRASPARSE || wf == WF_FAT) {
         // scan of the estimates: temporary slots per row, numeric classes by estimate
         st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s);
         OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
@@ -717,6 +735,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
       }
       if (wf == WF_PRECISE) {
         run_symbolic(h, A, B, s, readback, true, true);
+        mark("symbolic");
         nnz = h->h_ctr->total_nnz;
       } else {
         OCEAN_CUDA(cudaMallocAsync(&t_col, std::max<uint64_t>(st.total_est, 1) * 4, s));
@@ -726,7 +745,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
         const OutSpec est_out{h->w.est_off, h->w.est, h->w.cnt, h->w.ovf, &h->w.ctr->overflow_n};
         st.launches += launch_numeric(A, B, h->w, est_out, (uint32_t*)t_col, (double*)t_val, h->num_sms, s,
-                                      track ? h->ev + EV_NUM0 : nullptr, num_counts);
+                                      track ? h->ev + EV_NUM0 : nullptr, class_counts ? num_counts : nullptr);
         if (track) h->ev_mask |= ((1ull << (NB_COUNT + 1)) - 1) << EV_NUM0;
         // rows that did not fit their estimate: exact counts, then the row pointers
         st.launches += launch_overflow(A, B, h->w, false, nullptr, nullptr, h->num_sms, s);
@@ -735,6 +754,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
         OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
         check_device_status(h);
+        mark("estimated_numeric");
         nnz = h->h_ctr->total_nnz;
         st.overflow_rows = h->h_ctr->overflow_n;
         if (h->cfg.estimator_metrics && st.estimator != 0) measure_estimates(h, B, np, s);
@@ -749,6 +769,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     st.cache_words = h->w.bm_cache_words;
     st.cache_used = std::min<uint64_t>(h->h_ctr->cache_cursor, h->w.bm_cache_words);
     alloc_c(h, owner, A.rows, nnz, bits, s);
+    mark("alloc_c");
     if (A.rows > 0) {
       if (wf == WF_PRECISE) {
         unsigned num_counts[NB_COUNT];
@@ -776,10 +797,12 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     record(h, EV_END, s);
     h->ev_recorded = true;
     h->tracked = track;
+    mark("launched");
     if (h->cfg.sync_on_return && A.rows > 0) {
       OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
       OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
       check_device_status(h);
+      mark("synced");
     }
   } catch (...) {
     release_cache(h, s);
@@ -945,6 +968,10 @@ std::string stats_json(ocean_handle* h) {
       o << ", \"numeric_" << kNumNames[i] << "\": " << ev_ms(h, EV_NUM0 + i, EV_NUM0 + i + 1);
     o << ", \"host_ms\": " << st.host_ms << "}, ";
   }
+  o << "\"host_timeline_ms\": {";
+  for (size_t i = 0; i < st.host_marks.size(); ++i)
+    o << (i ? ", " : "") << "\"" << st.host_marks[i].first << "\": " << st.host_marks[i].second;
+  o << "}, ";
   o << "\"total_time\": " << total << ", \"gflops\": "
     << (total > 0 ? 2.0 * (double)st.total_products / total / 1e6 : 0.0) << "}";
   return o.str();

@@ -77,3 +77,17 @@ def test_direct_rows_fill_every_slot():
     C, _ = multiply_device(R, R, {"force_num_bin": NUM_BINS["hash_s"]})
     check(R, R, C)
     assert int(np.diff(C.rowptr.astype(np.int64)).max()) > 512
+
+
+@pytest.mark.parametrize("prefer", [True, False])
+def test_mid_rows_with_narrow_spans_take_a_direct_table(prefer):
+    # 512-wide bands of 32 entries: ~1000 outputs a row over ~1000 columns.
+    # With prefer_direct_hash (the default) the rows go to the 4096-slot class
+    # and are addressed directly; without it they go to the bitmap class.
+    A = M.banded(20000, 512, 32, seed=3)
+    C, st = multiply_device(A, A, {"prefer_direct_hash": prefer})
+    check(A, A, C)
+    b2 = st["binning_2"]
+    heavy = b2[NUM_BINS["hash_m"]] if prefer else b2[NUM_BINS["bitmap"]]
+    assert heavy > 0.9 * A.rows
+    assert st["host_timeline_ms"]["analysis"] <= st["host_timeline_ms"]["launched"]
