@@ -491,7 +491,10 @@ def run_ours(args, world, rank, local):
         parity = {"rows_checked_exact": len(set(check_rows)), "max_rel_err": worst, "tolerance": 1e-12,
                   "cpu_sample_row_counts_equal": counts_ok}
 
-    # ---- end to end through the host-buffer C ABI (pinned inputs, host output)
+    # ---- end to end through the host-buffer C ABI (pinned inputs, host output);
+    # the two device-input handles give back their workspaces and saved bitmaps first
+    g0.close()
+    g.close()
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(args, A, B, same, nnz_c, products, world, stream)

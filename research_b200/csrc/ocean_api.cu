@@ -1543,6 +1543,7 @@ int ocean_spgemm_host(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_
     }
     if (same) dv[1] = dv[0];
     ocean_csr dc;
+    const auto t_in = std::chrono::steady_clock::now();
     dispatch_spgemm(h, &dv[0], &dv[1], &dc, s);
     const uint64_t rpb = (dc.rows + 1) * (uint64_t)(dc.rowptr_bits / 8);
     CResult* dev_owner = (CResult*)dc._owner;
@@ -1567,6 +1568,9 @@ int ocean_spgemm_host(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_
     OCEAN_CUDA(cudaFreeAsync(dev_owner->val, s));
     delete dev_owner;
     OCEAN_CUDA(cudaStreamSynchronize(s));
+    // the copy-back on the multiply's host timeline (which starts at t_in)
+    h->st.host_marks.emplace_back(
+        "host_output_copied", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_in).count());
     *C = dc;
     C->rowptr = h->out_rp;
     C->col = h->out_col;
