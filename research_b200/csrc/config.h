@@ -200,6 +200,16 @@ struct Config {
   double bitmap_words_scale = 1.0;      // > 0: scales the column-span limits under which mid rows use bitmaps
   bool prefer_direct_hash = true;       // mid rows whose column span fits a hash table use it (direct slots)
   bool batch_autotune = false;          // batched plans: search the class policy on the batch before capturing
+  // segment-driven dispatch: rows of each spy-plot segment class take that
+  // class's policy (index = SegClass: sparse_uniform, dense, power_law, banded);
+  // unset fields inherit the global policy above
+  bool use_segment_dispatch = false;
+  int seg_esc_max_products[4] = {-1, -1, -1, -1};
+  double seg_hash_s_max_scale[4] = {0, 0, 0, 0};
+  double seg_bitmap_words_scale[4] = {0, 0, 0, 0};
+  int seg_prefer_direct_hash[4] = {-1, -1, -1, -1};
+  int seg_force_sym_bin[4] = {-2, -2, -2, -2};
+  int seg_force_num_bin[4] = {-2, -2, -2, -2};
 
   static Config from_json_text(const std::string& text) {
     Config c;
@@ -274,6 +284,29 @@ struct Config {
     getd("bitmap_words_scale", c.bitmap_words_scale);
     getb("prefer_direct_hash", c.prefer_direct_hash);
     getb("batch_autotune", c.batch_autotune);
+    getb("use_segment_dispatch", c.use_segment_dispatch);
+    static const char* kSegKey[4] = {"sparse_uniform", "dense", "power_law", "banded"};
+    for (int k = 0; k < 4; ++k) {
+      const std::string p = std::string("segment_") + kSegKey[k] + "_";
+      geti((p + "esc_max_products").c_str(), c.seg_esc_max_products[k]);
+      getd((p + "hash_s_max_scale").c_str(), c.seg_hash_s_max_scale[k]);
+      getd((p + "bitmap_words_scale").c_str(), c.seg_bitmap_words_scale[k]);
+      bool direct = c.seg_prefer_direct_hash[k] > 0;
+      const bool had = m.count(p + "prefer_direct_hash") > 0;
+      getb((p + "prefer_direct_hash").c_str(), direct);
+      if (had) c.seg_prefer_direct_hash[k] = direct ? 1 : 0;
+      geti((p + "force_sym_bin").c_str(), c.seg_force_sym_bin[k]);
+      geti((p + "force_num_bin").c_str(), c.seg_force_num_bin[k]);
+      if (c.seg_esc_max_products[k] < -1 || c.seg_esc_max_products[k] > 128)
+        throw std::invalid_argument(p + "esc_max_products must be in [0, 128]");
+      if (c.seg_hash_s_max_scale[k] < 0.0 || c.seg_hash_s_max_scale[k] > 1.0)
+        throw std::invalid_argument(p + "hash_s_max_scale must be in (0, 1]");
+      if (c.seg_bitmap_words_scale[k] < 0.0 || c.seg_bitmap_words_scale[k] > 64.0)
+        throw std::invalid_argument(p + "bitmap_words_scale must be in (0, 64]");
+      if (c.seg_force_sym_bin[k] < -2 || c.seg_force_sym_bin[k] > 6 || c.seg_force_num_bin[k] < -2 ||
+          c.seg_force_num_bin[k] > 6)
+        throw std::invalid_argument(p + "force_sym_bin / force_num_bin must be in [-1, 6]");
+    }
     if (c.output_rowptr_bits != 0 && c.output_rowptr_bits != 32 && c.output_rowptr_bits != 64)
       throw std::invalid_argument("output_rowptr_bits must be 0, 32 or 64");
     if (c.force_workflow < -1 || c.force_workflow > 3)

@@ -29,6 +29,9 @@ struct DevWork {
   unsigned long long* bm_cache = nullptr;  // exact column bitmaps saved by the symbolic pass
   uint64_t bm_cache_words = 0;   // capacity of bm_cache (0: no cache)
   DevCounters* ctr = nullptr;
+  // segment-driven dispatch: per-row policy slot (0: the call's policy,
+  // 1 + SegClass: that segment class's policy); null: slot 0 for every row
+  const uint8_t* row_pol = nullptr;
 };
 
 constexpr int kScanTile = 4096;
@@ -51,6 +54,16 @@ struct NumPolicy {
   uint32_t bm_words_m = 1024;
   uint32_t bm_words_l = 4096;
   uint32_t direct = 1;
+};
+
+// Policies of the dispatch slots (slot 0: the call's policy; 1..4: the
+// policies of the segment classes when segment-driven dispatch is on).
+constexpr int kPolicySlots = 5;
+struct SymPolicySet {
+  SymPolicy p[kPolicySlots];
+};
+struct NumPolicySet {
+  NumPolicy p[kPolicySlots];
 };
 
 // Symbolic class of a row from its product count and output column span.
@@ -79,7 +92,8 @@ __device__ __forceinline__ int num_bin_for(uint32_t n, uint64_t p, uint64_t span
 
 template <typename RP>
 int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
-                     cudaStream_t s);
+                     cudaStream_t s, const SymPolicy* seg = nullptr);
+// seg (optional): policies of the 4 segment classes, applied through w.row_pol.
 
 // bin_events (optional): SB_COUNT + 1 events recorded around the class kernels.
 // counts (optional): host copy of the rows per class; empty classes are not
@@ -93,7 +107,11 @@ int launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int nu
 // *total and out[rows]; with bin_rows, also appends every row to its numeric
 // class (chosen from in[] as the output count).
 int launch_scan(const DevWork& w, const uint32_t* in, uint64_t* out64, uint32_t* out32,
-                unsigned long long* total, bool bin_rows, const NumPolicy& pol, cudaStream_t s);
+                unsigned long long* total, bool bin_rows, const NumPolicy& pol, cudaStream_t s,
+                const NumPolicy* seg = nullptr);
+// Dispatch slots of the rows: 0 everywhere, then iv (n triples start, end,
+// slot of disjoint row intervals, device memory) painted over.
+void launch_paint_rows(const uint32_t* iv, uint32_t n, uint8_t* row_pol, uint64_t rows, cudaStream_t s);
 
 // HLL (estimation workflow): sketches of B's rows (2^log2p one-byte registers
 // each, into `sketch`) and the compaction statistics of the LCG-sampled rows

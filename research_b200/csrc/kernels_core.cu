@@ -108,7 +108,8 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
                                                   uint32_t* __restrict__ anz, uint32_t* __restrict__ maxb,
                                                   uint32_t* __restrict__ row_nnz, uint64_t* __restrict__ bm_off,
                                                   uint32_t* __restrict__ sym_bins,
-                                                  DevCounters* __restrict__ ctr, SymPolicy pol) {
+                                                  DevCounters* __restrict__ ctr, SymPolicySet pols,
+                                                  const uint8_t* __restrict__ row_pol) {
   __shared__ unsigned long long s_anz[SB_COUNT], s_prod[SB_COUNT], s_words;
   if (threadIdx.x < SB_COUNT) {
     s_anz[threadIdx.x] = 0ull;
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
       row_nnz[row] = 0;
     } else {
       const uint64_t span = (uint64_t)mx - mn + 1;
-      b = sym_bin_for(p, span, pol);
+      b = sym_bin_for(p, span, pols.p[row_pol ? row_pol[row] : 0]);
     }
   }
   {
@@ -1048,6 +1049,20 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------- segment dispatch
+// Writes each row's dispatch slot: block i paints rows [iv[3i], iv[3i+1]) with
+// slot iv[3i+2]. Intervals are disjoint; unpainted rows keep slot 0.
+__global__ void __launch_bounds__(256) k_paint_rows(const uint32_t* __restrict__ iv, uint8_t* __restrict__ row_pol) {
+  const uint32_t r0 = iv[3 * blockIdx.x], r1 = iv[3 * blockIdx.x + 1];
+  const uint8_t slot = (uint8_t)iv[3 * blockIdx.x + 2];
+  for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) row_pol[r] = slot;
+}
+
+void launch_paint_rows(const uint32_t* iv, uint32_t n, uint8_t* row_pol, uint64_t rows, cudaStream_t s) {
+  cudaMemsetAsync(row_pol, 0, rows, s);
+  if (n) k_paint_rows<<<n, 256, 0, s>>>(iv, row_pol);
+}
+
 // ---------------------------------------------------------------- scan
 __global__ void __launch_bounds__(1024) k_scan_reduce(const uint32_t* __restrict__ in, uint64_t n,
                                                       unsigned long long* __restrict__ tile_sums) {
@@ -1101,7 +1116,8 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
                                                      const uint32_t* __restrict__ anz,
                                                      const uint64_t* __restrict__ bm_off,
                                                      uint32_t* __restrict__ num_bins,
-                                                     DevCounters* __restrict__ ctr, NumPolicy pol, int bin_rows) {
+                                                     DevCounters* __restrict__ ctr, NumPolicySet pols,
+                                                     const uint8_t* __restrict__ row_pol, int bin_rows) {
   __shared__ unsigned long long scr[33];
   __shared__ unsigned long long s_cls[3][NB_COUNT];
   if (threadIdx.x < 3 * NB_COUNT) (&s_cls[0][0])[threadIdx.x] = 0ull;
@@ -1128,6 +1144,7 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
     }
     if (i < n && bin_rows) {
       const uint32_t p = prod[i];
+      const NumPolicy& pol = pols.p[row_pol ? row_pol[i] : 0];
       b = num_bin_for(v[q], p, (uint64_t)hi[i] - lo[i] + 1, pol);
       if (b >= 0 && pol.force_bin < 0 && bm_off[i] != ~0ull) b = NB_BITMAP;  // reuse the saved bitmap
 #pragma unroll
@@ -1411,17 +1428,20 @@ void configure_kernel_attributes() {
 
 template <typename RP>
 int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
-                    cudaStream_t s) {
+                    cudaStream_t s, const SymPolicy* seg) {
   if (A.rows == 0) return 0;
+  SymPolicySet pols;
+  for (int i = 0; i < kPolicySlots; ++i) pols.p[i] = (i > 0 && seg) ? seg[i - 1] : pol;
+  const uint8_t* row_pol = seg ? w.row_pol : nullptr;
   const double avg = (double)A.nnz / (double)A.rows;
   if (avg >= 12.0) {
     const uint64_t threads = A.rows * 32;
     k_analysis<RP, 32><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
+        A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pols, row_pol);
   } else {
     const uint64_t threads = A.rows * 4;
     k_analysis<RP, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pol);
+        A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pols, row_pol);
   }
   return 1;
 }
@@ -1481,13 +1501,17 @@ int launch_symbolic(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, int nu
 }
 
 int launch_scan(const DevWork& w, const uint32_t* in, uint64_t* out64, uint32_t* out32,
-                unsigned long long* total, bool bin_rows, const NumPolicy& pol, cudaStream_t s) {
+                unsigned long long* total, bool bin_rows, const NumPolicy& pol, cudaStream_t s,
+                const NumPolicy* seg) {
   const uint64_t nt = scan_tiles(w.rows);
   if (w.rows == 0) return 0;
+  NumPolicySet pols;
+  for (int i = 0; i < kPolicySlots; ++i) pols.p[i] = (i > 0 && seg) ? seg[i - 1] : pol;
+  const uint8_t* row_pol = seg ? w.row_pol : nullptr;
   k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(in, w.rows, w.tile_sums);
   k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, total, out64, out32, w.rows);
   k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(in, w.rows, w.tile_sums, out64, out32, w.prod, w.lo, w.hi, w.anz,
-                                             w.bm_off, w.num_bins, w.ctr, pol, bin_rows ? 1 : 0);
+                                             w.bm_off, w.num_bins, w.ctr, pols, row_pol, bin_rows ? 1 : 0);
   return 3;
 }
 
@@ -1612,9 +1636,9 @@ template int launch_overflow<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>
 template int launch_overflow<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, bool, uint32_t*,
                                        double*, int, cudaStream_t);
 template int launch_analysis<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
-                                        const SymPolicy&, cudaStream_t);
+                                        const SymPolicy&, cudaStream_t, const SymPolicy*);
 template int launch_analysis<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
-                                        const SymPolicy&, cudaStream_t);
+                                        const SymPolicy&, cudaStream_t, const SymPolicy*);
 template int launch_symbolic<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, int,
                                         cudaStream_t, cudaEvent_t*, const unsigned*);
 template int launch_symbolic<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, int,

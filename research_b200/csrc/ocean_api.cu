@@ -161,6 +161,17 @@ struct ocean_handle {
   // spy-plot segmentation of the last multiply (use_segmented_workflow)
   SegmentationResult seg;
   bool seg_ran = false;
+  // segment-driven dispatch of the last multiply: per-row slots, the
+  // segment-class policies, and the rows each slot received
+  uint8_t* row_pol = nullptr;
+  uint64_t row_pol_cap = 0;
+  uint32_t* seg_iv = nullptr;
+  uint64_t seg_iv_cap = 0;
+  SymPolicy seg_sp[4];
+  NumPolicy seg_np[4];
+  bool seg_dispatch = false;   // in force for the call under way (reset by every analysis)
+  bool seg_dispatched = false; // the last multiply was dispatched by segments (stats)
+  uint64_t seg_rows[kPolicySlots] = {0};
   // widened row pointers for mixed 32/64-bit inputs
   uint64_t* wide_a = nullptr;
   uint64_t wide_a_cap = 0;
@@ -198,6 +209,8 @@ struct ocean_handle {
     if (cache_buf) cudaFree(cache_buf);
     if (mlp_dev) cudaFree(mlp_dev);
     if (raw_est) cudaFree(raw_est);
+    if (row_pol) cudaFree(row_pol);
+    if (seg_iv) cudaFree(seg_iv);
     if (metrics_dev) cudaFree(metrics_dev);
     for (auto& e : ev) cudaEventDestroy(e);
   }
@@ -372,12 +385,36 @@ void make_policies(const Config& c, SymPolicy* sp, NumPolicy* np) {
   OCEAN_CHECK(sp->force_bin < SB_COUNT && np->force_bin < NB_COUNT, OCEAN_ERR_INVALID, "forced class out of range");
 }
 
+// Policies of the segment classes (SegClass order): the call's policies with
+// the class's configured fields in place of the global ones.
+void make_segment_policies(const Config& c, const SymPolicy& sp, const NumPolicy& np, SymPolicy* ssp,
+                           NumPolicy* snp) {
+  for (int k = 0; k < 4; ++k) {
+    Config ck = c;
+    if (c.seg_esc_max_products[k] >= 0) ck.esc_max_products = c.seg_esc_max_products[k];
+    if (c.seg_hash_s_max_scale[k] > 0.0) ck.hash_s_max_scale = c.seg_hash_s_max_scale[k];
+    if (c.seg_bitmap_words_scale[k] > 0.0) ck.bitmap_words_scale = c.seg_bitmap_words_scale[k];
+    if (c.seg_prefer_direct_hash[k] >= 0) ck.prefer_direct_hash = c.seg_prefer_direct_hash[k] > 0;
+    if (c.seg_force_sym_bin[k] >= -1) ck.force_sym_bin = c.seg_force_sym_bin[k];
+    if (c.seg_force_num_bin[k] >= -1) ck.force_num_bin = c.seg_force_num_bin[k];
+    make_policies(ck, &ssp[k], &snp[k]);
+  }
+  (void)sp;
+  (void)np;
+}
+
+// The segment policies in force for this call (null: no segment dispatch).
+const SymPolicy* seg_sym(const ocean_handle* h) { return h->seg_dispatch ? h->seg_sp : nullptr; }
+const NumPolicy* seg_num(const ocean_handle* h) { return h->seg_dispatch ? h->seg_np : nullptr; }
+
 // Phase 1: row analysis. Large inputs read the counters back (class sizes,
 // product totals); small inputs skip the read-back. Returns whether it read back.
 template <typename RP>
 bool run_analysis(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s) {
   h->ev_recorded = false;  // the stats describe a completed multiply only
   h->ev_mask = 0;
+  h->seg_dispatch = false;  // a call dispatches by segments only after its own segmentation
+  h->w.row_pol = nullptr;
   ensure_rows(h, A.rows);
   OCEAN_CUDA(cudaMemsetAsync(h->w.ctr, 0, sizeof(DevCounters), s));
   SymPolicy sp;
@@ -395,6 +432,72 @@ bool run_analysis(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStrea
     OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
   }
   return readback;
+}
+
+// Segment-driven dispatch: the segments' row bands become per-row policy
+// slots (slot 1 + SegClass; a row inside several bands takes the first band
+// listed; rows in no band keep slot 0, the call's policy); then the analysis
+// classes every row again under its slot's policy and, for inputs that read
+// back, the counters are read back again.
+template <typename RP>
+void dispatch_segments(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStream_t s, bool readback) {
+  SymPolicy sp;
+  NumPolicy np;
+  make_policies(h->cfg, &sp, &np);
+  make_segment_policies(h->cfg, sp, np, h->seg_sp, h->seg_np);
+  std::vector<uint32_t> iv;                               // start, end, slot triples
+  std::vector<std::pair<uint32_t, uint32_t>> taken;       // covered bands, sorted, disjoint
+  for (uint64_t i = 0; i < kPolicySlots; ++i) h->seg_rows[i] = 0;
+  for (const SegRecord& r : h->seg.segments) {
+    const uint32_t a = r.row_start;
+    const uint32_t b = (uint32_t)std::min<uint64_t>(r.row_end, A.rows);
+    if (a >= b || r.cls > SEG_BANDED) continue;
+    const uint32_t slot = 1 + r.cls;
+    uint32_t cur = a;
+    for (const auto& t : taken) {
+      if (t.second <= cur) continue;
+      if (t.first >= b) break;
+      if (t.first > cur) {
+        iv.insert(iv.end(), {cur, t.first, slot});
+        h->seg_rows[slot] += t.first - cur;
+      }
+      cur = std::max(cur, t.second);
+      if (cur >= b) break;
+    }
+    if (cur < b) {
+      iv.insert(iv.end(), {cur, b, slot});
+      h->seg_rows[slot] += b - cur;
+    }
+    taken.emplace_back(a, b);
+    std::sort(taken.begin(), taken.end());
+    std::vector<std::pair<uint32_t, uint32_t>> merged;
+    for (const auto& t : taken) {
+      if (!merged.empty() && t.first <= merged.back().second) merged.back().second = std::max(merged.back().second, t.second);
+      else merged.push_back(t);
+    }
+    taken.swap(merged);
+  }
+  uint64_t painted = 0;
+  for (int i = 1; i < kPolicySlots; ++i) painted += h->seg_rows[i];
+  h->seg_rows[0] = A.rows - painted;
+  const uint32_t n = (uint32_t)(iv.size() / 3);
+  grow(h->row_pol, h->row_pol_cap, A.rows);
+  if (n) {
+    grow(h->seg_iv, h->seg_iv_cap, iv.size());
+    // from pageable memory: the call returns once the triples are staged
+    OCEAN_CUDA(cudaMemcpyAsync(h->seg_iv, iv.data(), iv.size() * 4, cudaMemcpyHostToDevice, s));
+  }
+  launch_paint_rows(h->seg_iv, n, h->row_pol, A.rows, s);
+  h->w.row_pol = h->row_pol;
+  h->seg_dispatch = true;
+  h->seg_dispatched = true;
+  OCEAN_CUDA(cudaMemsetAsync(h->w.ctr, 0, sizeof(DevCounters), s));
+  h->st.launches += (n ? 1 : 0) + launch_analysis(A, B, h->w, sp, s, h->seg_sp);
+  OCEAN_CUDA(cudaGetLastError());
+  if (readback) {
+    OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+    OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
+  }
 }
 
 // Phase 2 of the precise workflow: symbolic class kernels (exact counts into
@@ -440,7 +543,8 @@ void run_symbolic(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStrea
   if (track && A.rows) h->ev_mask |= ((1ull << (SB_COUNT + 1)) - 1) << EV_SYM0;
   OCEAN_CUDA(cudaGetLastError());
   if (with_scan) {
-    h->st.launches += launch_scan(h->w, h->w.row_nnz, h->w.rowptr64, h->w.rowptr32, &h->w.ctr->total_nnz, true, np, s);
+    h->st.launches += launch_scan(h->w, h->w.row_nnz, h->w.rowptr64, h->w.rowptr32, &h->w.ctr->total_nnz, true, np, s,
+                                  seg_num(h));
     OCEAN_CUDA(cudaGetLastError());
   }
   if (track) record(h, EV_SCAN, s);
@@ -687,6 +791,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
   h->ev_recorded = false;
   h->ev_mask = 0;
   h->seg_ran = false;
+  h->seg_dispatched = false;
   const bool track = h->cfg.track_stage_times;
   NumPolicy np;
   {
@@ -703,13 +808,21 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     if (A.rows > 0) {
       const bool readback = run_analysis(h, A, B, s);
       mark("analysis");
-      if (h->cfg.use_segmented_workflow) {
-        // analysis-only pass: its records go to the stats (reference: kernels/SpGEMM.cuh:240-259)
+      if (h->cfg.use_segmented_workflow || h->cfg.use_segment_dispatch) {
+        // spy-plot segmentation; its records go to the stats (reference:
+        // kernels/SpGEMM.cuh:240-259, where it is analysis-only)
         const Config& c = h->cfg;
         OCEAN_CUDA(run_segmentation(A, B.cols, h->w, c.segmentation_grid_max, c.segmentation_hot_threshold_k,
                                     c.segmentation_min_segment_rows, c.segmentation_cc_max_iters,
                                     c.estimation_input_expansion_threshold, s, &h->seg));
         h->seg_ran = true;
+        if (c.use_segment_dispatch) {
+          // segment-driven dispatch (the reference's listed follow-up,
+          // kernels/SpGEMM.cuh:241-244): every row of a segment takes its
+          // class's policy, and the rows are classed again with them
+          dispatch_segments(h, A, B, s, readback);
+          mark("segment_dispatch");
+        }
       }
       wf = choose_workflow(h, A, B, s, readback);
       mark("workflow");
@@ -719,12 +832,14 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
       if (wf == WF_ULTRASPARSE && readback) {
         // the estimates are the product counts, whose total the analysis read
         // back and choose_workflow checked against free memory: no read-back
-        st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s);
+        st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s,
+                                   seg_num(h));
         st.total_est = h->h_ctr->total_products;
         class_counts = false;
       } else if (wf == WF_ESTIMATION || wf == WF_ULTRASPARSE || wf == WF_FAT) {
         // scan of the estimates: temporary slots per row, numeric classes by estimate
-        st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s);
+        st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s,
+                                   seg_num(h));
         OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
         OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
         st.total_est = h->h_ctr->total_est;
@@ -942,6 +1057,13 @@ std::string stats_json(ocean_handle* h) {
         << ", \"max_a_row_len\": " << r.max_a_row_len << "}";
     }
     o << "]}, ";
+  }
+  if (h->seg_dispatched) {
+    // rows per dispatch slot: outside every segment, then per segment class
+    o << "\"segment_dispatch\": {\"rows\": {\"unsegmented\": " << h->seg_rows[0];
+    static const char* kSegKey[4] = {"sparse_uniform", "dense", "power_law", "banded"};
+    for (int k = 0; k < 4; ++k) o << ", \"" << kSegKey[k] << "\": " << h->seg_rows[1 + k];
+    o << "}}, ";
   }
   o << "\"binning_1\": [";
   for (int i = 0; i < SB_COUNT; ++i) o << (i ? ", " : "") << st.sym_bins[i];

@@ -240,7 +240,7 @@ def plot_spy(matrix: str, stats: dict, mtx_path: Path, out: Path) -> None:
     seen = []
     for seg in stats.get("segmentation", {}).get("segments", []):
         cls = seg.get("class", "sparse_uniform")
-        color = CLASS_COLORS.get(cls, "#888888")
+        color = CLASS_COLORS.get(cls.lower(), "#888888")  # the stats spell classes in capitals
         sx = x0 + seg["col_left"] * scale
         sy = y0 + seg["row_start"] * scale
         sw = max(seg["col_right"] - seg["col_left"], 1) * scale
@@ -250,7 +250,7 @@ def plot_spy(matrix: str, stats: dict, mtx_path: Path, out: Path) -> None:
         if cls not in seen:
             seen.append(cls)
     for j, cls in enumerate(seen):
-        svg.rect(x0 + pw - 120, y0 + 8 + 16 * j, 10, 10, CLASS_COLORS.get(cls, "#888888"), cls="legend")
+        svg.rect(x0 + pw - 120, y0 + 8 + 16 * j, 10, 10, CLASS_COLORS.get(cls.lower(), "#888888"), cls="legend")
         svg.text(x0 + pw - 105, y0 + 17 + 16 * j, cls, size=10, anchor="start")
     svg.save(out)
 

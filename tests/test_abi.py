@@ -39,7 +39,9 @@ def test_version_and_error_string():
 
 
 @pytest.mark.parametrize("text", ['{"track_stage_time": ', '{"warmup_iters": "ten"}', '[1, 2]',
-                                  '{"output_rowptr_bits": 48}', '{"track_stage_time": true,, }'])
+                                  '{"output_rowptr_bits": 48}', '{"track_stage_time": true,, }',
+                                  '{"segment_dense_hash_s_max_scale": 2.0}', '{"segment_banded_esc_max_products": 500}',
+                                  '{"segment_power_law_force_num_bin": 9}', '{"segment_banded_prefer_direct_hash": "no"}'])
 def test_bad_config_is_invalid_status(text):
     L = ocean.lib()
     h = ctypes.c_void_p()
