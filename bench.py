@@ -491,6 +491,35 @@ def run_ours(args, world, rank, local):
         parity = {"rows_checked_exact": len(set(check_rows)), "max_rel_err": worst, "tolerance": 1e-12,
                   "cpu_sample_row_counts_equal": counts_ok}
 
+    # ---- the same product as a one-problem captured plan (ocean_batch_*): the
+    # repeated-structure form, whose launches replay a CUDA graph without the
+    # per-call read-backs; only where a second C fits easily beside the first
+    plan_line = None
+    if 12 * nnz_c < 8e9:
+        from research_b200.ocean import Batch
+        gb = SpGEMM({})
+        plan = Batch(gb, [dA], [dB], sptr)
+        for _ in range(args.warmup):
+            plan.launch(sptr)
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            plan.launch(sptr)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = max_over_ranks(p0.elapsed_time(p1), world) / args.steps
+        pinfo = plan.info()
+        out = plan.run(sptr)[0]
+        plan_same = int(out.nnz) == nnz_c
+        plan_line = {"value": round(world * 2.0 * products / (pms / 1e3) / 1e9, 3), "ms_per_step": round(pms, 4),
+                     "speedup_vs_plain": round(ms / pms, 3), "workflow": pinfo["workflow"],
+                     "kernel_launches": pinfo["kernel_launches"], "nnz_C_equal": plan_same,
+                     "api": "ocean_batch_create once, ocean_batch_launch per step (captured graph)"}
+        plan.close()
+        gb.close()
+
     # ---- end to end through the host-buffer C ABI (pinned inputs, host output);
     # the two device-input handles give back their workspaces and saved bitmaps first
     g0.close()
@@ -525,6 +554,8 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
         "parity": parity,
     }
+    if plan_line is not None:
+        line["captured_plan"] = plan_line
     print(json.dumps(line), flush=True)
 
 

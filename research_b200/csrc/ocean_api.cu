@@ -1283,10 +1283,13 @@ void batch_pipeline(ocean_batch* b, cudaStream_t s, bool plan) {
     b->products = k.total_products;
     const Config& c = b->cfg;
     const double avg = A.rows ? (double)k.total_products / (double)A.rows : 0.0;
+    // as for one product: ultra-sparse inputs are sized by their product
+    // counts (already exact upper bounds) before any estimator is asked
     if (c.force_workflow == WF_PRECISE) b->wf = WF_PRECISE;
-    else if (c.use_learned_estimator || c.force_workflow == WF_ESTIMATION) b->wf = WF_ESTIMATION;
+    else if (c.force_workflow == WF_ESTIMATION) b->wf = WF_ESTIMATION;
     else if (c.force_workflow == WF_ULTRASPARSE || (c.use_ultrasparse_workflow && avg <= c.usparse_avg_product_threshold))
       b->wf = WF_ULTRASPARSE;
+    else if (c.use_learned_estimator) b->wf = WF_ESTIMATION;
     else b->wf = WF_PRECISE;
     b->estimator = b->wf == WF_ESTIMATION ? (c.use_learned_estimator ? 2 : 1) : 0;
     if (b->estimator == 2) load_model(h);
