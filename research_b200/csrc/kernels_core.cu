@@ -352,8 +352,10 @@ __global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, RowQueue 
                                                  DevCounters* __restrict__ ctr, uint32_t* __restrict__ c_col,
                                                  double* __restrict__ c_val) {
   constexpr int CAP = 32 * K;
+  constexpr int LOGN = K == 1 ? 5 : (K == 2 ? 6 : 7);  // bits of a product's position in the warp
   __shared__ uint64_t s_src[8][CAP];
   __shared__ uint64_t s_aidx[8][CAP];
+  __shared__ double s_pval[8][CAP];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t count = *q.count;
   const uint32_t* list = q.rows;
@@ -374,7 +376,42 @@ __global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, RowQueue 
         val[e] = A.val[s_aidx[warp][i]] * B.val[sidx];
       }
     }
-    warp_bitonic_sort<K, true>(key, val);
+    // when the row's columns span less than 2^(32 - LOGN), the sort runs on
+    // one 32-bit word per product, (column - lo) << LOGN | position, and the
+    // values are fetched from shared memory by position afterwards: a third of
+    // the shuffles of sorting (column, value) pairs
+    uint32_t kmin = kEmpty, kmax = 0;
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+      kmin = min(kmin, key[e]);
+      if (key[e] != kEmpty) kmax = max(kmax, key[e]);
+    }
+    kmin = __reduce_min_sync(kFull, kmin);
+    kmax = __reduce_max_sync(kFull, kmax);
+    if (kmin == kEmpty || kmax - kmin < (1u << (32 - LOGN)) - 1u) {
+      uint32_t pk[K];
+#pragma unroll
+      for (int e = 0; e < K; ++e) {
+        const uint32_t pos = (uint32_t)(e << 5) | lane;
+        s_pval[warp][pos] = val[e];
+        pk[e] = key[e] == kEmpty ? kEmpty : ((key[e] - kmin) << LOGN) | pos;
+      }
+      __syncwarp();
+      warp_bitonic_sort<K, false>(pk, val);
+#pragma unroll
+      for (int e = 0; e < K; ++e) {
+        if (pk[e] == kEmpty) {
+          key[e] = kEmpty;
+          val[e] = 0.0;
+        } else {
+          key[e] = (pk[e] >> LOGN) + kmin;
+          val[e] = s_pval[warp][pk[e] & (CAP - 1)];
+        }
+      }
+      __syncwarp();
+    } else {
+      warp_bitonic_sort<K, true>(key, val);
+    }
     // segmented suffix sums inside each register row
 #pragma unroll
     for (int e = 0; e < K; ++e) {
