@@ -705,9 +705,11 @@ __global__ void __launch_bounds__(NT) k_sym_hash(Csr<RP> A, Csr<RP> B, RowQueue 
   }
 }
 
-// Numeric: hash-accumulate FP64 values in shared memory, compact the occupied
-// slots into (column << 32 | slot) keys, bitonic-sort them in shared memory and
-// write the row in column order directly into C.
+// Numeric: hash-accumulate FP64 values in shared memory, then write the row in
+// column order directly into C: rows whose span fits the table were addressed
+// directly and are compacted in slot order; the others are radix-sorted on
+// packed (column offset, dense index) words, or, when the span is too wide for
+// the packing, bitonic-sorted as (column << 32 | slot) keys.
 template <int NT, int LOG2T>
 struct NumHashSmem {
   double vals[1 << LOG2T];
