@@ -571,9 +571,20 @@ def run_e2e(args, A, B, same, nnz_c, products, world, stream):
                 avail = int(line.split()[1]) * 1024
     except Exception:
         pass
-    if avail and avail < need:
+    # every rank on this node pins its own copy of C: all of them must fit at
+    # once, and all ranks take the same decision (the leg has collectives)
+    local_world = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+    fits = not avail or avail >= need * local_world
+    if world > 1:
+        import torch.distributed as dist
+        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        flag = torch.tensor([1 if fits else 0], dtype=torch.int32, device=dev)
+        dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+        fits = bool(flag.item())
+    if not fits:
         return {"value": None, "unit": "GFLOP/s",
-                "note": f"skipped: host has {avail / 2**30:.0f} GiB available, needs {need / 2**30:.0f} GiB"}
+                "note": f"skipped: host has {avail / 2**30:.0f} GiB available, {local_world} rank(s) need "
+                        f"{need * local_world / 2**30:.0f} GiB of pinned memory"}
 
     def pinned(a: np.ndarray) -> np.ndarray:
         t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
