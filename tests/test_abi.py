@@ -2,6 +2,7 @@
 entry point declared in include/ocean.h; argument errors come back as status
 codes (no compute call is made without a GPU)."""
 import ctypes
+import json
 import re
 from pathlib import Path
 
@@ -76,6 +77,26 @@ def test_reference_config_files_parse_offline(tmp_path):
     h = ctypes.c_void_p()
     rc = L.ocean_create(ctypes.byref(h), text.encode())
     # without a GPU the parse succeeds and device setup fails with a CUDA status
+    assert rc in (0, 1), (rc, L.ocean_last_error())
+    if rc == 0:
+        L.ocean_destroy(h)
+
+
+def test_every_extra_config_key_parses():
+    """The keys this library adds are accepted with valid values."""
+    text = json.dumps({
+        "output_rowptr_bits": 64, "esc_max_products": 64, "hash_s_max_scale": 0.5, "bitmap_words_scale": 2.0,
+        "prefer_direct_hash": False, "bitmap_cache_fraction": 0.1, "small_problem_nnz": 0, "spin_wait_us": 100,
+        "force_workflow": 1, "estimate_scale": 1.5, "use_learned_estimator": True, "learned_estimator_weights": "",
+        "learned_margin_scale": 1.0, "estimator_metrics": True, "batch_autotune": True, "sync_on_return": False,
+        "use_segment_dispatch": True, "segment_sparse_uniform_esc_max_products": 32,
+        "segment_dense_hash_s_max_scale": 0.5, "segment_power_law_bitmap_words_scale": 4.0,
+        "segment_banded_prefer_direct_hash": True, "segment_dense_force_sym_bin": 6,
+        "segment_power_law_force_num_bin": -1, "fat_ratio": 50})
+    L = ocean.lib()
+    h = ctypes.c_void_p()
+    rc = L.ocean_create(ctypes.byref(h), text.encode())
+    # parsed and validated (without a GPU, creation then stops at the device: CUDA error)
     assert rc in (0, 1), (rc, L.ocean_last_error())
     if rc == 0:
         L.ocean_destroy(h)
