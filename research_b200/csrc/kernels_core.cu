@@ -10,8 +10,10 @@
 //   column sort             kernels/Epilogue.cuh:68-222 (CUB BlockRadixSort)
 //
 // Design: every row class runs as a persistent kernel whose blocks pull rows
-// from a device-side class list, so no bin count is read back to the host. The
-// only host read-back of a multiply is the total output count (to allocate C).
+// from a device-side class list, so the kernels need no bin count from the
+// host. The host reads back the class sizes after the analysis (large inputs
+// only, to size the grids and the bitmap cache) and the total output count
+// (to allocate C).
 // Numeric kernels write each row already sorted straight into its final place
 // in C, so there is no temporary output buffer and no separate sort/copy pass.
 #include <algorithm>
