@@ -1,12 +1,29 @@
 """The reference's own CUDA build (oracle/_ref/spgemm_ref, compiled from the
-reference sources by `make -C oracle refbin`) run on the 2D Laplacian 256x256
-C = A*A input, with its ground-truth comparison (src/CSR.cpp:252-335) pointed at
-the CPU oracle's C. This pins the oracle to the reference's actual output
-(exact row offsets and column ids, values within the reference's 1e-4 hard
-limit) and records the reference's GFLOP/s beside this library's on the same
-input. Only this input is run: its reference path (ultra-sparse workflow, ESC
-kernel of size 32, CUB scans, copy) was read and has no unbounded waits."""
+reference sources by `make -C oracle refbin` with NUM_SM = 148) run on inputs
+whose reference code path was read first and has no unbounded waits, with its
+ground-truth comparison (src/CSR.cpp:252-335) pointed at the CPU oracle's C.
+This pins the oracle to the reference's actual output (exact row offsets and
+column ids, values within the reference's 1e-4 hard limit) and records the
+reference's time beside this library's on the same input.
+
+Inputs and the reference path each one takes:
+  * 2D Laplacian 256x256, C = A*A: ultra-sparse workflow, ESC kernel of size
+    32, CUB scans, copy (kernels/Wrappers.cuh:440-470).
+  * rectangular 262144 x 1048576, Poisson(12) per row, C = A*A^T: ultra-sparse
+    workflow, kernel size 64, hashNumericSubWarpKernel<4, 80> for rows of at
+    most 64 products and hashNumericKernel<6, 331> for the outliers (at most
+    131 products here, kernels/Wrappers.cuh:282-322,422-473). Both tables hold
+    more slots than the rows have products, so their probe loops
+    (kernels/Hashmap.cuh:56-78) always find a free slot.
+  * four row bands (banded, uniform, block-diagonal, R-MAT with at most 40
+    entries per row; at most 838 products and 825 outputs per row): workflow
+    with the spy-plot segmentation (kernels/SpGEMM.cuh:240-258), whose loops
+    are bounded by segmentation_cc_max_iters and 8 pointer-jumping rounds
+    (kernels/Segmentation.cuh:496-519); every row fits the smallest shared
+    hash tables, so no global-buffer pool (kernels/AccumulatorCommon.cuh:8-31)
+    is used. The segmentation records are compared with this library's."""
 import json
+import math
 import os
 import subprocess
 from pathlib import Path
@@ -15,6 +32,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from oracle import segmentation as S
 from research_b200 import matrices as M
 from research_b200.ocean import DeviceCSR, HostCSR, SpGEMM
 
@@ -24,41 +42,163 @@ REF = ROOT / "oracle" / "_ref" / "spgemm_ref"
 pytestmark = pytest.mark.gpu
 
 
-def test_reference_build_agrees_with_oracle_on_laplacian(tmp_path):
+def _need_ref():
     if not REF.exists():
         pytest.skip("reference driver not built (make -C oracle refbin needs the reference source tree)")
-    A = M.laplacian_2d(256, 256, seed=0)
-    pa = tmp_path / "lap256.mtxd_.hicsr"
-    M.write_hicsr(A, pa)
-    cp, cj, cx = O.spgemm(A, A)
-    pt = tmp_path / "truth.mtxd_.hicsr"
-    M.write_hicsr(HostCSR(A.rows, A.cols, cp.astype(np.uint32), cj, cx), pt)
-    stats = tmp_path / "ref_stats.json"
-    cfg = tmp_path / "bench.json"
-    cfg.write_text(json.dumps({"warmup_iters": 10, "bench_iters": 10, "check_correctness": True,
-                               "ground_truth_file": str(pt), "output_stats": True,
-                               "stats_output_file": str(stats), "print_info": False,
-                               "track_stage_time": False}))
-    r = subprocess.run([str(REF), str(pa), str(cfg)], capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
-    assert "Comparison completed" in r.stdout
-    ref = json.loads(stats.read_text())
-    assert ref["C"]["nnz"] == int(cp[-1])
-    # this library on the same input, same iteration counts
-    g = SpGEMM({"track_stage_time": False})
-    dA = DeviceCSR.from_host(A)
-    ms = []
-    for i in range(20):
-        C = g.multiply(dA, dA)
-        if i >= 10:
-            ms.append(g.stage_ms("total"))
-        C.free()
-    ours = 2.0 * 1629192 / (sum(ms) / len(ms)) / 1e6
-    rec = {"input": "laplacian 256x256, C=A*A", "reference_gflops": ref["gflops"],
-           "reference_ms": ref["total_time"], "reference_workflow": ref["decision"]["workflow"],
-           "ours_gflops": ours, "ours_ms": sum(ms) / len(ms)}
+
+
+def _record(name: str, rec: dict):
     print(json.dumps(rec))
     out = os.environ.get("OCEAN_RECORD_DIR")
     if out:
         Path(out).mkdir(parents=True, exist_ok=True)
-        (Path(out) / "reference_gpu_laplacian.json").write_text(json.dumps(rec) + "\n")
+        (Path(out) / f"reference_gpu_{name}.json").write_text(json.dumps(rec) + "\n")
+
+
+def run_reference(tmp_path, A, B, extra=None, iters=(10, 10)):
+    """Runs the reference driver on A*B with its correctness check against the
+    oracle's C; returns (stats dict, stdout, oracle C rowptr)."""
+    pa = tmp_path / "a.mtxd_.hicsr"
+    M.write_hicsr(A, pa)
+    args = [str(REF), str(pa)]
+    if B is not A:
+        pb = tmp_path / "b.mtxd_.hicsr"
+        M.write_hicsr(B, pb)
+        args.append(str(pb))
+    cp, cj, cx = O.spgemm(A, B)
+    pt = tmp_path / "truth.mtxd_.hicsr"
+    M.write_hicsr(HostCSR(A.rows, B.cols, cp.astype(np.uint32), cj, cx), pt)
+    stats = tmp_path / "ref_stats.json"
+    cfg = tmp_path / "bench.json"
+    cfg.write_text(json.dumps({"warmup_iters": iters[0], "bench_iters": iters[1], "check_correctness": True,
+                               "ground_truth_file": str(pt), "output_stats": True,
+                               "stats_output_file": str(stats), "print_info": False,
+                               "track_stage_time": False, **(extra or {})}))
+    args.append(str(cfg))
+    r = subprocess.run(args, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "Comparison completed" in r.stdout
+    ref = json.loads(stats.read_text())
+    assert ref["C"]["nnz"] == int(cp[-1])
+    return ref, r.stdout, cp
+
+
+def ours_ms(A, B, iters=(10, 10), config=None):
+    """This library's mean multiply time (ms) over the timed iterations, device inputs."""
+    g = SpGEMM({"track_stage_time": False, **(config or {})})
+    dA = DeviceCSR.from_host(A)
+    dB = dA if B is A else DeviceCSR.from_host(B)
+    ms = []
+    for i in range(iters[0] + iters[1]):
+        C = g.multiply(dA, dB)
+        if i >= iters[0]:
+            ms.append(g.stage_ms("total"))
+        C.free()
+    st = g.get_stats()
+    g.close()
+    return sum(ms) / len(ms), st
+
+
+def test_reference_build_agrees_with_oracle_on_laplacian(tmp_path):
+    _need_ref()
+    A = M.laplacian_2d(256, 256, seed=0)
+    ref, _, _ = run_reference(tmp_path, A, A)
+    ms, st = ours_ms(A, A)
+    products = int(st["stats"]["intermediate_product"])
+    _record("laplacian", {"input": "laplacian 256x256, C=A*A", "num_sm": 148, "reference_gflops": ref["gflops"],
+                          "reference_ms": ref["total_time"], "reference_workflow": ref["decision"]["workflow"],
+                          "ours_gflops": 2.0 * products / ms / 1e6, "ours_ms": ms})
+
+
+def test_reference_build_agrees_with_oracle_on_rectangular(tmp_path):
+    _need_ref()
+    A = M.rect_poisson(262144, 1048576, 12.0, seed=0)
+    B = M.transpose(A)
+    p, _, _ = O.row_stats(A, B)
+    assert int(p.max()) <= 160, "input outside the path read for this test"
+    ref, out, cp = run_reference(tmp_path, A, B)
+    ms, st = ours_ms(A, B)
+    products = int(st["stats"]["intermediate_product"])
+    assert products == int(ref["stats"]["intermediate_product"])
+    _record("rect", {"input": "262144x1048576 Poisson(12), C=A*A^T", "num_sm": 148,
+                     "reference_gflops": ref["gflops"], "reference_ms": ref["total_time"],
+                     "reference_workflow": ref["decision"]["workflow"], "nnz_C": int(cp[-1]),
+                     "ours_gflops": 2.0 * products / ms / 1e6, "ours_ms": ms})
+
+
+def mixed_bands(n: int = 65536, seed: int = 11, cap: int = 40):
+    """Four row bands of n/4 rows each taken from a banded, a uniform, a
+    block-diagonal and an R-MAT matrix (rows of the R-MAT band cut to their
+    first `cap` entries)."""
+    q = n // 4
+    parts = [M.banded(n, 33, 24, seed=seed), M.uniform_random(n, 20, seed=seed + 1),
+             M.block_diagonal(n, 256, 24, seed=seed + 2), M.rmat(16, 4, seed=seed + 3)]
+    rows, cols, vals = [], [], []
+    for i, P in enumerate(parts):
+        rp = P.rowptr.astype(np.int64)
+        lo, hi = i * q, (i + 1) * q
+        s, e = rp[lo], rp[hi]
+        lens = np.diff(rp[lo:hi + 1])
+        r = np.repeat(np.arange(lo, hi), lens)
+        keep = (np.arange(s, e) - np.repeat(rp[lo:hi], lens)) < cap
+        rows.append(r[keep])
+        cols.append(P.col[s:e].astype(np.int64)[keep])
+        vals.append(P.val[s:e][keep])
+    return M.from_coo(n, n, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals))
+
+
+SEG_CONFIGS = [
+    dict(segmentation_grid_max=64, segmentation_hot_threshold_k=1.0, segmentation_min_segment_rows=1024),
+    dict(segmentation_grid_max=256, segmentation_hot_threshold_k=2.0, segmentation_min_segment_rows=256),
+]
+EXACT_SEG = ["row_start", "row_end", "row_count", "col_left", "col_right", "class", "sum_products", "sum_a_nnz",
+             "max_b_row_len", "max_a_row_len"]
+FLOAT_SEG = ["mean_row_len", "var_row_len", "local_er"]
+
+
+def _close(a, b, rel=1e-9):
+    return a == b or abs(a - b) <= rel * max(abs(a), abs(b))
+
+
+@pytest.mark.parametrize("cfg", SEG_CONFIGS, ids=["grid64_k1", "grid256_k2"])
+def test_segmentation_records_match_reference_build(tmp_path, cfg):
+    """Spy-plot segmentation: the reference build's records against this
+    library's (and the CPU restatement's) on the same input and keys.
+    cc_iterations is not compared: the reference's label propagation reads
+    labels other threads are writing, so its round count depends on timing;
+    the converged labels, the component count and the segments do not."""
+    _need_ref()
+    A = mixed_bands()
+    p, _, _ = O.row_stats(A, A)
+    assert int(p.max()) <= 1000 and p.mean() > 64, "input outside the path read for this test"
+    ref, _, _ = run_reference(tmp_path, A, A, extra={"use_segmented_workflow": True, **cfg}, iters=(0, 1))
+    assert "segmentation" in ref, "reference did not run its segmentation"
+    g = SpGEMM({"use_segmented_workflow": True, "output_stats": True, **cfg})
+    g.multiply(A, A)
+    ours = g.get_stats()["segmentation"]
+    want = S.segment(A, A, grid_max=cfg["segmentation_grid_max"], hot_k=cfg["segmentation_hot_threshold_k"],
+                     min_segment_rows=cfg["segmentation_min_segment_rows"])
+    rs = ref["segmentation"]
+    diffs = []
+    for f in ("grid_h", "grid_w", "tile_rows", "tile_cols", "num_components"):
+        if rs[f] != ours[f]:
+            diffs.append((f, rs[f], ours[f]))
+    for f in ("density_mean", "density_stddev"):
+        if not _close(rs[f], ours[f]):
+            diffs.append((f, rs[f], ours[f]))
+    if len(rs["segments"]) != len(ours["segments"]):
+        diffs.append(("segments", len(rs["segments"]), len(ours["segments"])))
+    else:
+        for i, (a, b) in enumerate(zip(rs["segments"], ours["segments"])):
+            for f in EXACT_SEG:
+                if a[f] != b[f]:
+                    diffs.append((f"segments[{i}].{f}", a[f], b[f]))
+            for f in FLOAT_SEG:
+                if not _close(a[f], b[f]):
+                    diffs.append((f"segments[{i}].{f}", a[f], b[f]))
+    _record(f"segmentation_{cfg['segmentation_grid_max']}",
+            {"input": "four row bands, n=65536", "config": cfg, "segments": len(rs["segments"]),
+             "reference_cc_iterations": rs["cc_iterations"], "ours_cc_iterations": ours["cc_iterations"],
+             "differences": diffs[:20]})
+    assert not diffs, diffs[:20]
+    assert ours["segments"] == want["segments"]
