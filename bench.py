@@ -293,24 +293,31 @@ def cpu_gustavson(A, B, threads: int, chunk_products: int = 300_000_000):
     return time.perf_counter() - t0, int(prod.sum()), counts
 
 
-def cpu_sample(A, B, threads: int, target_s: float = 12.0):
-    """Bounded CPU sample: every s-th row of A, s chosen so the run takes about
-    target_s seconds. Returns dict with the measured rate and the sample."""
-    total_rows = A.rows
-    s = 256
-    rows = np.arange(0, total_rows, s)
-    t, p, _ = cpu_gustavson(take_rows(A, rows), B, threads)
-    rate = p / max(t, 1e-6)
+CPU_SAMPLE_PRODUCTS = 2.3e9  # products of one CPU sample (about 5 s of OpenMP Gustavson on 16 cores)
+
+
+def cpu_sample_rows(A, B, threads: int):
+    """The rows of the bounded CPU sample, the same for the reference arm and
+    the cpu_baseline leg: every s-th row of A, s = round(products /
+    CPU_SAMPLE_PRODUCTS) (all rows when the product is smaller)."""
     from oracle import oracle as O
     prod_all, _, _ = O.row_stats(A, B, threads)
     total = float(prod_all.sum())
-    frac = min(1.0, target_s * rate / max(total, 1.0))
-    s = max(1, int(round(1.0 / max(frac, 1e-9))))
-    rows = np.arange(0, total_rows, s)
+    s = max(1, int(round(total / CPU_SAMPLE_PRODUCTS)))
+    return np.arange(0, A.rows, s), s, int(total)
+
+
+def cpu_sample(A, B, threads: int, repeats: int = 2):
+    """The bounded CPU sample timed `repeats` times (symbolic + numeric each)."""
+    rows, s, _ = cpu_sample_rows(A, B, threads)
     sub = take_rows(A, rows)
-    t, p, counts = cpu_gustavson(sub, B, threads)
-    return {"seconds": t, "products": p, "stride": s, "rows": rows, "counts": counts,
-            "gflops": 2.0 * p / t / 1e9}
+    t_all, p_all, counts = 0.0, 0, None
+    for _ in range(max(1, repeats)):
+        t, p, counts = cpu_gustavson(sub, B, threads)
+        t_all += t
+        p_all += p
+    return {"seconds": t_all, "products": p_all // max(1, repeats), "stride": s, "rows": rows, "counts": counts,
+            "repeats": max(1, repeats), "gflops": 2.0 * p_all / t_all / 1e9}
 
 
 # ----------------------------------------------------------------------------- dist
@@ -353,15 +360,9 @@ def run_reference(args, world, rank):
         return
     A, B, desc = make_workload(args.workload)
     threads = os.cpu_count() or 1
-    from oracle import oracle as O
-    prod_all, _, _ = O.row_stats(A, B, threads)
-    total = int(prod_all.sum())
-    # calibrate the stride on a small sample, then time K bounded samples
-    cal = cpu_sample(A, B, threads, target_s=max(2.0, args.ref_seconds))
-    rows = cal["rows"]
+    rows, stride, total = cpu_sample_rows(A, B, threads)
     sub = take_rows(A, rows)
-    for _ in range(max(0, args.warmup - 1)):
-        pass  # the calibration run above is the warm-up
+    cpu_gustavson(sub, B, threads)  # one untimed run: page cache and thread pool warm
     times, prods = [], []
     for _ in range(args.steps):
         t, p, _ = cpu_gustavson(sub, B, threads)
@@ -375,7 +376,7 @@ def run_reference(args, world, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": desc, "rows": A.rows, "nnz_A": A.nnz, "products": total},
         "cpu_baseline": {"value": round(value, 4), "unit": "GFLOP/s", "cores": threads, "kind": "port",
-                         "sample": f"every {cal['stride']}th row of A ({rows.size} rows, {prods[0]} products "
+                         "sample": f"every {stride}th row of A ({rows.size} rows, {prods[0]} products "
                                    f"per step), symbolic+numeric OpenMP Gustavson (oracle/gustavson.c)"},
         "e2e": {"value": round(value, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference has no CPU SpGEMM; this arm times the project's CPU restatement of its "
@@ -397,7 +398,7 @@ def run_ours(args, world, rank, local):
     # ---- CPU baseline first (host memory is still free), rank 0 at N=1 only
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(A, B, os.cpu_count() or 1, target_s=args.cpu_seconds)
+        cpu = cpu_sample(A, B, os.cpu_count() or 1, repeats=args.cpu_repeats)
 
     # ---- device-resident throughput (a handle without stage events)
     g0 = SpGEMM({})
@@ -528,6 +529,12 @@ def run_ours(args, world, rank, local):
     if not args.no_e2e:
         e2e = run_e2e(args, A, B, same, nnz_c, products, world, stream)
 
+    configs = None
+    if world == 1 and not args.no_extra:
+        del dA, dB
+        torch.cuda.empty_cache()
+        configs = extra_legs(args, stream)
+
     if rank != 0:
         return
     line = {
@@ -547,8 +554,9 @@ def run_ours(args, world, rank, local):
                      "launch_ms": round(stage_ms[dom], 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
         "cpu_baseline": None if cpu is None else {
             "value": round(cpu["gflops"], 4), "unit": "GFLOP/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"every {cpu['stride']}th row of A ({cpu['rows'].size} rows, {cpu['products']} products), "
-                      f"symbolic+numeric OpenMP Gustavson, {cpu['seconds']:.1f} s"},
+            "sample": f"every {cpu['stride']}th row of A ({cpu['rows'].size} rows, {cpu['products']} products; "
+                      f"the reference arm's sample), symbolic+numeric OpenMP Gustavson, {cpu['repeats']} runs, "
+                      f"{cpu['seconds']:.1f} s"},
         "e2e": e2e,
         "gpu_launches": int(st["decision"].get("kernel_launches", KERNELS_PER_MULTIPLY)) * args.steps,
         "clocks": clk,
@@ -556,6 +564,8 @@ def run_ours(args, world, rank, local):
     }
     if plan_line is not None:
         line["captured_plan"] = plan_line
+    if configs is not None:
+        line["configs"] = configs
     print(json.dumps(line), flush=True)
 
 
@@ -626,212 +636,274 @@ def run_e2e(args, A, B, same, nnz_c, products, world, stream):
             "api": "ocean_spgemm_host (pinned host A/B in, C copied back to pinned host buffers)"}
 
 
-def run_batch(args, world, rank, local):
-    """Workload batch512: 512 independent A_p*A_p (n log-uniform 1k-64k; banded,
-    R-MAT, uniform and block-diagonal in turn; 4-32 entries per row; FP64;
-    generated on the device, seed 5). The learned estimator and the class-policy
-    autotuner are on; one step is one launch of the captured graph of the
-    whole batch. Beside it, the plain form: 512 sequential ocean_spgemm calls
-    per step. e2e: pinned host inputs copied in, the graph, every result copied
-    back (ocean_batch_download); plain e2e: 512 ocean_spgemm_host calls."""
+# ----------------------------------------------------------------------------- further configs
+# The default run also measures the metric's other forms on one GPU, each with
+# its own fixed, small step counts so the whole run stays within minutes:
+# configs 1 and 3 (Laplacian 256^2 and the rectangular A*A^T) as plain calls,
+# as a one-problem captured plan and end to end; config 4 (learned row sizing
+# of the held-out R-MAT 2^21 against HLL and exact counts); config 5 (512
+# products: learned + batched against 512 plain calls, with the HLL- and
+# exact-sized batched forms beside it, on the device and end to end).
+
+def _ev():
+    import torch
+    return torch.cuda.Event(enable_timing=True)
+
+
+def time_on_device(fn, steps: int, warmup: int, stream) -> float:
+    """Mean ms per call of fn() over `steps` calls after `warmup`, CUDA events on `stream`."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = _ev(), _ev()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def leg_small(name: str, stream, steps: int = 20, warmup: int = 5, check: bool = True) -> dict:
+    import torch
+    from research_b200.ocean import Batch, CsrOut, DeviceCSR, SpGEMM, _check, lib
+    A, B, desc = make_workload(name)
+    same = B is A
+    sptr = stream.cuda_stream
+    dA = DeviceCSR.from_host(A)
+    dB = dA if same else DeviceCSR.from_host(B)
+    g = SpGEMM({})
+    plain_ms = time_on_device(lambda: g.multiply(dA, dB, sptr).free(sptr), steps, warmup, stream)
+    st = g.get_stats()
+    products, nnz_c = int(st["stats"]["intermediate_product"]), int(st["C"]["nnz"])
+    out = {"workload": desc, "products": products, "nnz_C": nnz_c, "workflow": st["decision"]["workflow"],
+           "plain_ms": round(plain_ms, 4), "plain_gflops": round(2.0 * products / plain_ms / 1e6, 3),
+           "kernel_launches": st["decision"]["kernel_launches"]}
+    if check:
+        from oracle import oracle as O
+        C = g.multiply(dA, dB, sptr)
+        h = C.download()
+        C.free(sptr)
+        cp, cj, cx, ca = O.spgemm(A, B, with_abs=True)
+        out["parity_max_rel_err"] = O.compare(h.rowptr, h.col, h.val, cp, cj, cx, ca, 1e-12)
+    gb = SpGEMM({})
+    plan = Batch(gb, [dA], [dB], sptr)
+    plan_ms = time_on_device(lambda: plan.launch(sptr), steps, warmup, stream)
+    out["captured_plan_ms"] = round(plan_ms, 4)
+    out["captured_plan_launches"] = plan.info()["kernel_launches"]
+    plan.close()
+    gb.close()
+    # end to end: pinned host inputs, C copied back (ocean_spgemm_host)
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(a.dtype)[: a.size]
+        v[:] = a
+        pinned.keep.append(t)
+        return v
+    pinned.keep = []
+    from research_b200.ocean import HostCSR
+    pA = HostCSR(A.rows, A.cols, pinned(A.rowptr), pinned(A.col), pinned(A.val))
+    pB = pA if same else HostCSR(B.rows, B.cols, pinned(B.rowptr), pinned(B.col), pinned(B.val))
+    av, bv = pA.view(), pB.view()
+    res = CsrOut()
+    e2e_ms = time_on_device(lambda: _check(lib().ocean_spgemm_host(g._h, ctypes.byref(av), ctypes.byref(bv),
+                                                                   ctypes.byref(res), sptr)),
+                            steps, warmup, stream)
+    out["e2e_ms"] = round(e2e_ms, 4)
+    out["e2e_gflops"] = round(2.0 * products / e2e_ms / 1e6, 3)
+    g.close()
+    return out
+
+
+def leg_sizing(stream, steps: int = 3, warmup: int = 2) -> dict:
+    """Config 4: row sizes of C = A*A for the held-out R-MAT n = 2^21 (24 per
+    row, seed 7; generated on the device; C, ~0.55 TB, is never formed) by
+    exact symbolic counts, HLL and the learned network, with the estimates'
+    errors against the exact counts on the rows they size (> 128 products)."""
     import torch
     from research_b200 import estimator as E
-    from research_b200.ocean import Batch, CsrOut, SpGEMM, _check, lib
-    torch.cuda.set_device(local)
-    stream = torch.cuda.current_stream()
+    from research_b200.ocean import SpGEMM
+    A = E.generate("rmat", 1 << 21, 24, seed=7)
+    g = SpGEMM({})
+    truth = g.symbolic(A, A)
+    exact_ms = time_on_device(lambda: g.symbolic(A, A), steps, warmup, stream)
+    res = {}
+    for name in ("learned", "hll"):
+        ms = time_on_device(lambda: E.estimate(g, A, None, name, True), steps, warmup, stream)
+        est = E.estimate(g, A, None, name, True)
+        raw = E.estimate(g, A, None, name, False)
+        res[name] = {"ms": round(ms, 3), "prealloc": E.metrics(g, est, truth, 128), "raw": E.metrics(g, raw, truth, 128)}
+    g.close()
+    return {"workload": "R-MAT n=2^21, 24 entries/row, seed 7 (held out from training); row sizes of C=A*A",
+            "rows": A.rows, "nnz_A": A.nnz, "exact_symbolic_ms": round(exact_ms, 3), "learned": res["learned"],
+            "hll": res["hll"], "speedup_learned_vs_exact": round(exact_ms / res["learned"]["ms"], 2),
+            "speedup_learned_vs_hll": round(res["hll"]["ms"] / res["learned"]["ms"], 3)}
+
+
+def leg_batch(stream, steps: int = 3, warmup: int = 2, e2e_steps: int = 2, ablation: bool = True,
+              check: bool = True) -> dict:
+    """Config 5: 512 independent A_p*A_p (n log-uniform 1k-64k; banded, R-MAT,
+    uniform and block-diagonal in turn; 4-32 entries per row; FP64; generated
+    on the device, seed 5). Plain: 512 sequential ocean_spgemm calls. Learned +
+    batched: one captured graph of the whole batch, rows sized by the network,
+    class policy autotuned. Ablation: the same batched graph sized by HLL, and
+    by exact symbolic counts. End to end: pinned host inputs copied in, every
+    result copied back (batched: ocean_batch_download; plain: 512
+    ocean_spgemm_host calls)."""
+    import torch
+    from research_b200 import estimator as E
+    from research_b200.ocean import Batch, CsrOut, HostCSR, SpGEMM, _check, lib
     sptr = stream.cuda_stream
     specs = E.training_specs(512, seed=5, n_lo=1024, n_hi=65536)
     dA = [E.generate(sp.kind, sp.n, sp.deg, sp.seed, sp.param) for sp in specs]
     torch.cuda.synchronize()
-    ev = lambda: torch.cuda.Event(enable_timing=True)
-
-    # plain: one ocean_spgemm per problem
     gp = SpGEMM({})
     products = 0
     for a in dA:
         C = gp.multiply(a, a, sptr)
         products += int(gp.get_stats()["stats"]["intermediate_product"])
         C.free(sptr)
-    for _ in range(max(0, args.warmup - 1)):
+
+    def plain_step():
         for a in dA:
             gp.multiply(a, a, sptr).free(sptr)
-    e0, e1 = ev(), ev()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        for a in dA:
-            gp.multiply(a, a, sptr).free(sptr)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1) / args.steps
+    plain_ms = time_on_device(plain_step, steps, warmup, stream)
+    gf = lambda ms: round(2.0 * products / (ms / 1e3) / 1e9, 3)
+    out = {"workload": "512 x A_p*A_p, n log-uniform 1k-64k, banded/R-MAT/uniform/block-diagonal in turn, "
+                       "4-32 entries per row, FP64 U[-1,1], seed 5", "products": products,
+           "plain": {"ms": round(plain_ms, 3), "gflops": gf(plain_ms), "form": "512 sequential ocean_spgemm calls"}}
 
-    # learned + batched: one graph launch per step
-    gb = SpGEMM({"use_learned_estimator": True, "batch_autotune": True})
-    t0 = time.time()
-    plan = Batch(gb, dA, stream=sptr)
-    plan_s = time.time() - t0
-    info = plan.info()
-    for _ in range(args.warmup):
-        plan.launch(sptr)
-    plan.run(sptr)  # checked launch
-    clocks = clock_sampler(local)
-    clocks.start()
-    e0, e1 = ev(), ev()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        plan.launch(sptr)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    batch_ms = e0.elapsed_time(e1) / args.steps
-    res = plan.run(sptr)
+    def batched(config):
+        gb = SpGEMM(config)
+        t0 = time.time()
+        plan = Batch(gb, dA, stream=sptr)
+        plan_s = time.time() - t0
+        ms = time_on_device(lambda: plan.launch(sptr), steps, warmup, stream)
+        return gb, plan, ms, plan_s
 
-    parity = None
-    if not args.no_check:
-        from oracle import oracle as O
-        worst = 0.0
-        for p in list(range(0, 512, 37)):
-            h = res[p].download()
-            A = dA[p].download()
-            rp, cj, cx, ca = O.spgemm(A, A, with_abs=True)
-            worst = max(worst, O.compare(h.rowptr, h.col, h.val, rp, cj, cx, ca, 1e-12))
-        parity = {"problems_checked": len(range(0, 512, 37)), "max_rel_err": worst, "tolerance": 1e-12}
+    forms = [("learned_batched", {"use_learned_estimator": True, "batch_autotune": True})]
+    if ablation:
+        forms += [("hll_batched", {"force_workflow": 1}), ("exact_batched", {"force_workflow": 0})]
+    for name, cfg in forms:
+        gb, plan, ms, plan_s = batched(cfg)
+        info = plan.info()
+        rec = {"ms": round(ms, 3), "gflops": gf(ms), "speedup_vs_plain": round(plain_ms / ms, 3),
+               "plan_seconds": round(plan_s, 2), "kernel_launches": info["kernel_launches"],
+               "workflow": info["workflow"], "estimator": info.get("estimator"), "nnz_C": int(info["nnz_c"])}
+        if name == "learned_batched":
+            rec["tuning"] = info.get("tuning")
+            res = plan.run(sptr)
+            if check:
+                from oracle import oracle as O
+                worst = 0.0
+                for q in range(0, 512, 37):
+                    h = res[q].download()
+                    A = dA[q].download()
+                    rp, cj, cx, ca = O.spgemm(A, A, with_abs=True)
+                    worst = max(worst, O.compare(h.rowptr, h.col, h.val, rp, cj, cx, ca, 1e-12))
+                rec["parity"] = {"problems_checked": len(range(0, 512, 37)), "max_rel_err": worst}
+            if e2e_steps > 0:
+                rec["e2e"] = batch_e2e(plan, info, dA, gp, stream, e2e_steps)
+                out["plain"]["e2e_ms"] = rec["e2e"].pop("plain_ms")
+                out["plain"]["e2e_gflops"] = gf(out["plain"]["e2e_ms"])
+                rec["e2e"]["gflops"] = gf(rec["e2e"]["ms"])
+                rec["e2e_speedup_vs_plain"] = round(out["plain"]["e2e_ms"] / rec["e2e"]["ms"], 3)
+        out[name] = rec
+        plan.close()
+        gb.close()
+    gp.close()
+    return out
 
-    # e2e (pinned host copies of every input and of the stacked result)
-    avail = 0
-    try:
-        for ln in open("/proc/meminfo"):
-            if ln.startswith("MemAvailable:"):
-                avail = int(ln.split()[1]) * 1024
-    except Exception:
-        pass
-    need = 12 * int(info["nnz_c"]) + 24 * int(info["nnz_a"]) + (8 << 30)
-    if avail and avail < need:
-        print(json.dumps({"note": f"e2e skipped: {avail / 2**30:.0f} GiB host memory available, "
-                                  f"{need / 2**30:.0f} GiB needed"}), file=sys.stderr)
-        args.e2e_steps = 0
+
+def batch_e2e(plan, info, dA, gp, stream, steps: int) -> dict:
+    """End-to-end ms of one batched step and of 512 plain host-buffer calls."""
+    import torch
+    from research_b200.ocean import CsrOut, HostCSR, _check, lib
+    sptr = stream.cuda_stream
 
     def pinned_like(t):
         return torch.empty(t.shape, dtype=t.dtype, pin_memory=True).copy_(t.cpu())
-    if args.e2e_steps <= 0:
-        raise SystemExit("batch512 needs --e2e-steps >= 1 and enough host memory")
     hosts = [(pinned_like(a.rowptr), pinned_like(a.col), pinned_like(a.val)) for a in dA]
     nnz_c = int(info["nnz_c"])
     rows_tot = int(info["rows"])
-    rp_out = torch.empty(rows_tot + 512, dtype=torch.int64 if info["rowptr_bits"] == 64 else torch.int32,
+    rp_out = torch.empty(rows_tot + len(dA), dtype=torch.int64 if info["rowptr_bits"] == 64 else torch.int32,
                          pin_memory=True)
     col_out = torch.empty(max(nnz_c, 1), dtype=torch.int32, pin_memory=True)
     val_out = torch.empty(max(nnz_c, 1), dtype=torch.float64, pin_memory=True)
-    h2d = sum(x.nbytes for hs in hosts for x in hs)
-    d2h = rp_out.nbytes + 12 * nnz_c
 
-    def e2e_step():
+    def step():
         for a, (r, c, v) in zip(dA, hosts):
             a.rowptr.copy_(r, non_blocking=True)
             a.col.copy_(c, non_blocking=True)
             a.val.copy_(v, non_blocking=True)
         plan.launch(sptr)
         plan.download_into(rp_out.numpy(), col_out.numpy(), val_out.numpy(), sptr)
-    e2e_step()
-    e0, e1 = ev(), ev()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.e2e_steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    ms = time_on_device(step, steps, 1, stream)
+    hcsr = [HostCSR(a.rows, a.cols, r.numpy().view(np.uint32) if a.rowptr_bits == 32 else r.numpy().view(np.uint64),
+                    c.numpy().view(np.uint32), v.numpy()) for a, (r, c, v) in zip(dA, hosts)]
+    res = CsrOut()
 
-    # plain e2e: 512 host-buffer calls
-    from research_b200.ocean import HostCSR
-    hcsr = [HostCSR(a.rows, a.cols, r.numpy().view(np.uint32), c.numpy().view(np.uint32), v.numpy())
-            for a, (r, c, v) in zip(dA, hosts)]
-    out = CsrOut()
-    for m in hcsr:
-        mv = m.view()
-        _check(lib().ocean_spgemm_host(gp._h, ctypes.byref(mv), ctypes.byref(mv), ctypes.byref(out), sptr))
-    e0, e1 = ev(), ev()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.e2e_steps):
+    def plain():
         for m in hcsr:
             mv = m.view()
-            _check(lib().ocean_spgemm_host(gp._h, ctypes.byref(mv), ctypes.byref(mv), ctypes.byref(out), sptr))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    plain_e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+            _check(lib().ocean_spgemm_host(gp._h, ctypes.byref(mv), ctypes.byref(mv), ctypes.byref(res), sptr))
+    plain_ms = time_on_device(plain, steps, 1, stream)
+    return {"ms": round(ms, 3), "plain_ms": round(plain_ms, 3),
+            "h2d_bytes_per_step": int(sum(x.nbytes for hs in hosts for x in hs)),
+            "d2h_bytes_per_step": int(rp_out.nbytes + 12 * nnz_c),
+            "api": "pinned host inputs -> device, ocean_batch_launch, ocean_batch_download; "
+                   "plain: 512 x ocean_spgemm_host"}
 
-    gf = lambda ms: round(2.0 * products / (ms / 1e3) / 1e9, 3)
-    line = {
-        "metric": METRIC + " (batch of 512 independent products)", "value": gf(batch_ms), "unit": "GFLOP/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(batch_ms, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "batch512: 512 x A_p*A_p, n log-uniform 1k-64k, banded/R-MAT/uniform/block-diagonal "
-                               "in turn, 4-32 entries per row, FP64 U[-1,1], seed 5",
-                   "rows": rows_tot, "nnz_A": int(info["nnz_a"]), "nnz_C": nnz_c, "products": products,
-                   "l2": "inputs and outputs (%.1f GB) larger than L2" % ((12 * int(info["nnz_a"]) + 12 * nnz_c) / 1e9)},
-        "plain": {"value": gf(plain_ms), "ms_per_step": round(plain_ms, 3),
-                  "form": "512 sequential ocean_spgemm calls (device inputs)"},
-        "speedup_vs_plain": round(plain_ms / batch_ms, 3),
-        "plan": {"seconds": round(plan_s, 3), **info},
-        "e2e": {"value": gf(e2e_ms), "unit": "GFLOP/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "ms_per_step": round(e2e_ms, 3),
-                "api": "pinned host inputs -> device buffers, ocean_batch_launch, ocean_batch_download"},
-        "plain_e2e": {"value": gf(plain_e2e_ms), "ms_per_step": round(plain_e2e_ms, 3),
-                      "api": "512 x ocean_spgemm_host"},
-        "e2e_speedup_vs_plain": round(plain_e2e_ms / e2e_ms, 3),
-        "gpu_launches": int(info["kernel_launches"]) * args.steps,
-        "clocks": clk, "parity": parity,
-    }
+
+def extra_legs(args, stream) -> dict:
+    out = {}
+    for name, fn in (("laplacian256", lambda: leg_small("laplacian256", stream, check=not args.no_check)),
+                     ("rect", lambda: leg_small("rect", stream, check=not args.no_check)),
+                     ("rmat21_sizing", lambda: leg_sizing(stream)),
+                     ("batch512", lambda: leg_batch(stream, check=not args.no_check,
+                                                     e2e_steps=0 if args.no_e2e else 2))):
+        t0 = time.time()
+        try:
+            out[name] = fn()
+        except Exception as e:  # report, keep the headline line
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["leg_seconds"] = round(time.time() - t0, 1)
+        import torch
+        torch.cuda.empty_cache()
+    return out
+
+
+
+def run_batch(args, world, rank, local):
+    """Workload batch512 alone (config 5): see leg_batch."""
+    import torch
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    clocks = clock_sampler(local)
+    clocks.start()
+    r = leg_batch(stream, steps=args.steps, warmup=args.warmup, e2e_steps=0 if args.no_e2e else args.e2e_steps,
+                  check=not args.no_check)
+    clk = clocks.stop()
+    lb = r["learned_batched"]
+    line = {"metric": METRIC + " (batch of 512 independent products)", "value": lb["gflops"], "unit": "GFLOP/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": lb["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batch512: " + r["workload"], "products": r["products"]},
+            "e2e": None if "e2e" not in lb else {"value": lb["e2e"]["gflops"], "unit": "GFLOP/s",
+                                                 "h2d_bytes_per_step": lb["e2e"]["h2d_bytes_per_step"],
+                                                 "d2h_bytes_per_step": lb["e2e"]["d2h_bytes_per_step"]},
+            "gpu_launches": int(lb["kernel_launches"]) * args.steps, "clocks": clk, "batch512": r}
     print(json.dumps(line), flush=True)
-    plan.close()
 
 
 def run_sizing(args, world, rank, local):
-    """Workload rmat21-sizing: the held-out R-MAT (n = 2^21, 24 entries per
-    row, seed 7; generated on the device) whose C (~0.5 TB) is never formed.
-    Times the three ways of sizing every output row: exact symbolic counts
-    (plain precise workflow), HLL estimates (the reference's estimation
-    workflow) and the learned network; and scores the estimates against the
-    exact counts on the rows they size (> 128 products)."""
+    """Workload rmat21-sizing alone (config 4): see leg_sizing."""
     import torch
-    from research_b200 import estimator as E
-    from research_b200.ocean import SpGEMM
     torch.cuda.set_device(local)
-    A = E.generate("rmat", 1 << 21, 24, seed=7)
-    g = SpGEMM({})
-    ev = lambda: torch.cuda.Event(enable_timing=True)
-    stream = torch.cuda.current_stream()
-
-    def timed(fn):
-        for _ in range(args.warmup):
-            fn()
-        torch.cuda.synchronize()
-        e0, e1 = ev(), ev()
-        e0.record(stream)
-        for _ in range(args.steps):
-            out = fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / args.steps, out
-
-    exact_ms, truth = timed(lambda: g.symbolic(A, A))
-    res = {}
-    for name in ("learned", "hll"):
-        ms, est = timed(lambda: E.estimate(g, A, None, name, True))
-        m = E.metrics(g, est, truth, 128)
-        m["est_total"] = int((est.to(torch.int64) & 0xFFFFFFFF).sum().item())
-        raw = E.estimate(g, A, None, name, False)
-        mr = E.metrics(g, raw, truth, 128)
-        res[name] = {"ms": round(ms, 3), "prealloc": m, "raw": mr}
-    line = {"workload": "rmat21-sizing: R-MAT n=2^21, 24 entries/row, seed 7; row sizes of C=A*A",
-            "rows": A.rows, "nnz_A": A.nnz, "truth_total": int((truth.to(torch.int64) & 0xFFFFFFFF).sum().item()),
-            "exact_symbolic_ms": round(exact_ms, 3), "learned": res["learned"], "hll": res["hll"],
-            "speedup_learned_vs_exact": round(exact_ms / res["learned"]["ms"], 2),
-            "speedup_learned_vs_hll": round(res["hll"]["ms"] / res["learned"]["ms"], 3),
-            "steps": args.steps, "warmup": args.warmup}
-    print(json.dumps(line), flush=True)
+    r = leg_sizing(torch.cuda.current_stream(), steps=args.steps, warmup=args.warmup)
+    r["steps"], r["warmup"] = args.steps, args.warmup
+    print(json.dumps(r), flush=True)
 
 
 def main():
@@ -842,11 +914,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat20")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--cpu-repeats", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="headline workload only (no configs 1, 3, 4, 5)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("note: fewer than 3 warm-up steps", file=sys.stderr)

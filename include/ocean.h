@@ -126,8 +126,9 @@ int ocean_row_estimates(ocean_handle* h, const ocean_csr_view* A, const ocean_cs
  * so A may have at most 131072 rows (larger A: OCEAN_ERR_INVALID). A and B need
  * the same row-pointer width; row_nnz[A.rows] is the caller's device array. The
  * first call on a device resolves the array's address and must come before any
- * stream capture. Calls share the array: calls that overlap on the GPU race and
- * must be ordered by the caller. Waits for the result before returning.
+ * stream capture; the address is kept, so a cudaDeviceReset after that first
+ * call is not supported. Calls share the array: calls that overlap on the GPU
+ * race and must be ordered by the caller. Waits for the result before returning.
  * No counterpart in the reference (which allocates on every run). */
 int ocean_symbolic_noalloc(const ocean_csr_view* A, const ocean_csr_view* B, uint32_t* row_nnz,
                            void* stream);

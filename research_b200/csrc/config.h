@@ -199,6 +199,7 @@ struct Config {
   double hash_s_max_scale = 1.0;        // (0, 1]: fill limit of the small hash tables relative to the default
   double bitmap_words_scale = 1.0;      // > 0: scales the column-span limits under which mid rows use bitmaps
   bool prefer_direct_hash = true;       // mid rows whose column span fits a hash table use it (direct slots)
+  bool numeric_windows = false;         // exact numeric bitmap class: shared-memory value windows (k_num_window)
   bool batch_autotune = false;          // batched plans: search the class policy on the batch before capturing
   // segment-driven dispatch: rows of each spy-plot segment class take that
   // class's policy (index = SegClass: sparse_uniform, dense, power_law, banded);
@@ -283,6 +284,7 @@ struct Config {
     getd("hash_s_max_scale", c.hash_s_max_scale);
     getd("bitmap_words_scale", c.bitmap_words_scale);
     getb("prefer_direct_hash", c.prefer_direct_hash);
+    getb("numeric_windows", c.numeric_windows);
     getb("batch_autotune", c.batch_autotune);
     getb("use_segment_dispatch", c.use_segment_dispatch);
     static const char* kSegKey[4] = {"sparse_uniform", "dense", "power_law", "banded"};

@@ -29,6 +29,15 @@ struct DevWork {
   unsigned long long* bm_cache = nullptr;  // exact column bitmaps saved by the symbolic pass
   uint64_t bm_cache_words = 0;   // capacity of bm_cache (0: no cache)
   DevCounters* ctr = nullptr;
+  // exact-mode numeric bitmap class (k_num_window): resume cursor per A entry
+  // (capacity >= nnz(A) when some row of the class has more than 1024 A
+  // entries), a 2^20-bit bitmap per block for rows without a saved bitmap, and
+  // the host's count of the class's rows wider than 2^20 columns (kUnknownCount:
+  // not known, the kernel for them is launched anyway). Null buffers: the class
+  // runs in k_num_bitmap alone.
+  uint32_t* win_cursor = nullptr;
+  unsigned long long* win_scratch = nullptr;
+  uint32_t wide_rows = 0xFFFFFFFFu;
   // segment-driven dispatch: per-row policy slot (0: the call's policy,
   // 1 + SegClass: that segment class's policy); null: slot 0 for every row
   const uint8_t* row_pol = nullptr;
@@ -150,8 +159,15 @@ void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t se
 // out[r] = min(products, column span) for every row of the last analysis.
 int launch_row_bounds(const DevWork& w, uint32_t* out, cudaStream_t s);
 
-// Per-kernel dynamic shared memory opt-in; call once per device.
+// Per-kernel dynamic shared memory opt-in and occupancy table; call once per
+// device, with it current (ensure_kernel_attributes does so under a lock, for
+// every entry point that may be first on a device; false: bad ordinal).
 void configure_kernel_attributes();
+bool ensure_kernel_attributes(int dev);
+
+// Words of DevWork::win_scratch for a device with num_sms SMs (one 2^20-bit
+// bitmap per resident block of k_num_window); valid after configure_kernel_attributes.
+size_t window_scratch_words(int num_sms);
 
 // Stores the calling thread's error message returned by ocean_last_error().
 void set_last_error(const char* msg);

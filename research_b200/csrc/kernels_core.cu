@@ -18,6 +18,7 @@
 // in C, so there is no temporary output buffer and no separate sort/copy pass.
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 #include "kernels.h"
 
 namespace ocean {
@@ -513,20 +514,12 @@ struct EnumSmem {
 #endif
 constexpr int kUnroll = OCEAN_UNROLL;  // gathers in flight per thread in the product enumeration
 
-// Loads A entries [c0, min(c0 + NT, a1)) into E (compacted to non-empty B rows).
-template <int NT, bool VALS, typename RP>
-__device__ __forceinline__ void block_load_chunk(const Csr<RP>& A, const Csr<RP>& B, uint64_t c0, uint64_t a1,
+// Packs one B-row range per thread (start bs, length len, A value av) into E,
+// compacted to the non-empty ranges.
+template <int NT, bool VALS>
+__device__ __forceinline__ void block_pack_chunk(unsigned long long bs, unsigned long long len, double av,
                                                  EnumSmem<NT>& E) {
   const int tid = threadIdx.x;
-  const uint64_t k = c0 + tid;
-  unsigned long long len = 0, bs = 0;
-  double av = 0.0;
-  if (k < a1) {
-    const uint32_t j = A.col[k];
-    bs = B.row_begin(j);
-    len = B.row_end(j) - bs;
-    if (VALS) av = A.val[k];
-  }
   // packed scan: high 16 bits count non-empty rows, low 48 bits sum products
   const unsigned long long packed = len ? ((1ull << 48) | len) : 0ull;
   unsigned long long tot;
@@ -544,6 +537,22 @@ __device__ __forceinline__ void block_load_chunk(const Csr<RP>& A, const Csr<RP>
     E.total = tot & kLow;
   }
   __syncthreads();
+}
+
+// Loads A entries [c0, min(c0 + NT, a1)) into E (compacted to non-empty B rows).
+template <int NT, bool VALS, typename RP>
+__device__ __forceinline__ void block_load_chunk(const Csr<RP>& A, const Csr<RP>& B, uint64_t c0, uint64_t a1,
+                                                 EnumSmem<NT>& E) {
+  const uint64_t k = c0 + threadIdx.x;
+  unsigned long long len = 0, bs = 0;
+  double av = 0.0;
+  if (k < a1) {
+    const uint32_t j = A.col[k];
+    bs = B.row_begin(j);
+    len = B.row_end(j) - bs;
+    if (VALS) av = A.val[k];
+  }
+  block_pack_chunk<NT, VALS>(bs, len, av, E);
 }
 
 // Enumerates the products of the chunk held in E. `op(col, value, ok)` is
@@ -987,6 +996,64 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, RowQueue 
   }
 }
 
+// Emits the set bits of one 64-bit word per lane (a warp's group of 32
+// consecutive bitmap words) in rank order: emit(j, b) for the group's j-th set
+// bit, at bit offset b from the group's first bit. Sparse groups (at most
+// kSparseBits bits in every word) are written by a per-lane loop over each
+// word's bits (lanes write nearly consecutive entries); denser groups entry by
+// entry, lane l taking entries l, l + 32, ..., the owner word found by a
+// binary search over the lanes' exclusive counts and the bit by a 6-step
+// select. Warp-collective; emit runs on the lanes that own an entry.
+constexpr uint32_t kSparseBits = 8;
+template <typename Emit>
+__device__ __forceinline__ void warp_emit_group(unsigned long long word, int lane, Emit&& emit) {
+  const uint32_t cnt = (uint32_t)__popcll(word);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int sh = 1; sh < 32; sh <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, sh);
+    if (lane >= sh) incl += y;
+  }
+  const uint32_t excl = incl - cnt;
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return;
+  if (__reduce_max_sync(kFull, cnt) <= kSparseBits) {
+    uint32_t j = excl;
+    unsigned long long x = word;
+    while (x) {
+      const uint32_t b = (uint32_t)(__ffsll((long long)x) - 1);
+      x &= x - 1ull;
+      emit(j++, (uint32_t)lane * 64u + b);
+    }
+    return;
+  }
+  const uint32_t rounds = (total + 31) >> 5;
+  for (uint32_t rd = 0; rd < rounds; ++rd) {
+    const uint32_t j = rd * 32 + lane;
+    uint32_t k = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const uint32_t e = __shfl_sync(kFull, excl, k + step);
+      if (e <= j) k += step;
+    }
+    unsigned long long x = __shfl_sync(kFull, word, k);
+    uint32_t r = j - __shfl_sync(kFull, excl, k);
+    if (j < total) {
+      uint32_t pos = 0;
+#pragma unroll
+      for (int sb = 32; sb > 0; sb >>= 1) {
+        const uint32_t c = (uint32_t)__popcll(x & ((1ull << sb) - 1ull));
+        if (r >= c) {
+          r -= c;
+          x >>= sb;
+          pos += sb;
+        }
+      }
+      emit(j, k * 64u + pos);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- bitmap accumulators
 // Symbolic: a bitmap over (a window of) the row's output column span; the count
 // is the popcount. Windows of 2^20 columns sweep wider spans.
@@ -1077,7 +1144,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
                  const uint32_t* __restrict__ prod, const uint32_t* __restrict__ lo,
                  const uint32_t* __restrict__ hi, const uint64_t* __restrict__ bm_off,
                  const unsigned long long* __restrict__ cache, uint32_t* __restrict__ c_col,
-                 double* __restrict__ c_val) {
+                 double* __restrict__ c_val, bool wide_only) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BitmapNumSmem& S = *reinterpret_cast<BitmapNumSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1091,6 +1158,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
   // Spread, few heavy rows run together (R-MAT 2^20: 280 -> 225 ms).
   const uint32_t stride = spread_stride(count);
   for (;;) {
+    __syncthreads();  // every thread has read the previous row index
     if (tid == 0) S.s_idx = atomicAdd(q.cursor, 1u);
     __syncthreads();
     const uint32_t idx = S.s_idx;
@@ -1098,6 +1166,7 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
     const uint32_t row = list[spread_index(idx, count, stride)];
     const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
     const uint64_t rlo = lo[row], rhi = hi[row];
+    if (wide_only && rhi - rlo + 1 <= kBitmapBits) continue;  // k_num_window's rows
     const uint64_t row_off = o.off[row];
     const uint32_t expect = o.cap[row];
     const uint64_t row_lim = row_off + expect;
@@ -1170,54 +1239,19 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
         run += __shfl_sync(kFull, x, 31);
       }
       __syncthreads();
-      // ordered output of the column ids (and zeroed values): each warp takes
-      // 32-word groups; the group's entries are written in rank order, lane l
-      // writing entries l, l + 32, ... (coalesced): the owner word of an entry
-      // is found by a binary search over the lanes' exclusive counts, its bit
-      // by a 6-step select on the word
+      // ordered output of the column ids (and zeroed values), a warp per
+      // group of 32 words
       for (uint32_t wb = (uint32_t)warp * 32u; wb < nwords; wb += 32u * (kBitmapThreads / 32)) {
         const uint32_t w = wb + lane;
-        const unsigned long long word = w < nwords ? S.bits[w] : 0ull;
-        const uint32_t cnt = (uint32_t)__popcll(word);
-        uint32_t incl = cnt;
-#pragma unroll
-        for (int sh = 1; sh < 32; sh <<= 1) {
-          const uint32_t y = __shfl_up_sync(kFull, incl, sh);
-          if (lane >= sh) incl += y;
-        }
-        const uint32_t excl = incl - cnt;
-        const uint32_t total = __shfl_sync(kFull, incl, 31);
-        if (total == 0) continue;
-        const uint32_t gpre = S.spre[wb >> 10] + S.wpre[wb];
-        const uint32_t rounds = (total + 31) >> 5;
-        for (uint32_t rd = 0; rd < rounds; ++rd) {
-          const uint32_t j = rd * 32 + lane;
-          uint32_t k = 0;
-#pragma unroll
-          for (int step = 16; step > 0; step >>= 1) {
-            const uint32_t e = __shfl_sync(kFull, excl, k + step);
-            if (e <= j) k += step;
+        const uint64_t gout = off + S.spre[wb >> 10] + S.wpre[wb];
+        const uint64_t gcol = w0 + (uint64_t)wb * 64;
+        warp_emit_group(w < nwords ? S.bits[w] : 0ull, lane, [&](uint32_t j, uint32_t b) {
+          const uint64_t o = gout + j;
+          if (o < row_lim) {
+            c_col[o] = (uint32_t)(gcol + b);
+            c_val[o] = 0.0;
           }
-          unsigned long long x = __shfl_sync(kFull, word, k);
-          uint32_t r = j - __shfl_sync(kFull, excl, k);
-          if (j < total) {
-            uint32_t pos = 0;
-#pragma unroll
-            for (int sb = 32; sb > 0; sb >>= 1) {
-              const uint32_t c = (uint32_t)__popcll(x & ((1ull << sb) - 1ull));
-              if (r >= c) {
-                r -= c;
-                x >>= sb;
-                pos += sb;
-              }
-            }
-            const uint64_t o = off + gpre + j;
-            if (o < row_lim) {
-              c_col[o] = (uint32_t)(w0 + (uint64_t)(wb + k) * 64 + pos);
-              c_val[o] = 0.0;
-            }
-          }
-        }
+        });
       }
       __syncthreads();
       // pass 2: accumulate values at their ranks
@@ -1236,6 +1270,259 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       __syncthreads();
     }
     if (tid == 0 && !o.count && off != row_lim) raise_status(ctr, DEV_COUNT_MISMATCH, row);
+  }
+}
+
+// ---------------------------------------------------------------- windowed numeric accumulator
+// Exact-mode numeric kernel of the bitmap class, for rows whose column span
+// fits one 2^20-bit bitmap. The row's exact output bitmap (saved by the
+// symbolic pass, or marked here into a per-block scratch copy) is swept in
+// windows of whole words holding at most kWinV output entries and kWinWords
+// words. For each window the block loads the window's bitmap words and their
+// exclusive popcounts into shared memory, finds every A entry's run of its
+// sorted B row inside the window's column range (a resume cursor per A entry
+// marks where the previous window stopped, so every B entry of the row is
+// enumerated once over the whole sweep), accumulates the products into FP64
+// slots in shared memory at the window-local rank of their column, and writes
+// the window's column ids and values to C once, in order. There is no global
+// atomic and no zero-fill of C; the reference's denseNumericIterKernel
+// (kernels/AccumulatorDense.cuh:610-806) sweeps column windows the same way
+// with dense per-column slots, which this kernel replaces by bitmap ranks so
+// that sparse wide rows take few windows.
+constexpr int kWinV = 12288;     // output entries per window (FP64 slots in shared memory)
+constexpr int kWinWords = 8192;  // bitmap words per window (512K columns)
+static_assert(kWinV + kWinWords >= kBitmapWords, "the marking bitmap overlays the slots and window words");
+static_assert(kWinV < 65536, "window-local ranks are 16-bit");
+
+struct WinNumSmem {
+  unsigned long long area[kWinV + kWinWords];  // FP64 slots, then the window's words; marking: the row bitmap
+  uint16_t wpre[kWinWords];                    // exclusive popcount of the window's words before each word
+  EnumSmem<kBitmapThreads> e;
+  unsigned long long seg_pos[64], seg_end[64];  // few-entry chunks: B-run starts / row ends, then run ends
+  uint32_t scan[33];
+  uint32_t s_idx, s_we, s_nwin;
+};
+
+// First index p in [lo, hi) with col[p] >= cb (hi when there is none); col is
+// sorted on [lo, hi). Warp-collective: the first round checks the first 32
+// entries, later rounds probe 32 evenly spaced entries of the remaining range.
+__device__ __forceinline__ uint64_t warp_run_end(const uint32_t* __restrict__ col, uint64_t lo, uint64_t hi,
+                                                 uint32_t cb) {
+  const int lane = threadIdx.x & 31;
+  for (int round = 0; round < 24 && lo < hi; ++round) {
+    const uint64_t n = hi - lo;
+    if (round == 0 || n <= 32) {
+      const uint64_t p = lo + lane;
+      const bool ge = p < hi && col[p] >= cb;
+      const unsigned m = __ballot_sync(kFull, ge);
+      if (m) return lo + (uint64_t)(__ffs(m) - 1);
+      if (n <= 32) return hi;
+      lo += 32;
+      continue;
+    }
+    const uint64_t step = (n + 31) / 32;
+    const uint64_t q = lo + (uint64_t)(lane + 1) * step - 1;
+    const bool ge = q < hi ? col[q] >= cb : true;
+    const unsigned m = __ballot_sync(kFull, ge);
+    const int f = __ffs(m) - 1;  // lane 31 probes at or past hi - 1: m == 0 only if col[hi - 1] < cb
+    if (f < 0) return hi;
+    const uint64_t nhi = min(lo + (uint64_t)(f + 1) * step - 1, hi);
+    lo = lo + (uint64_t)f * step;
+    hi = nhi;
+  }
+  return hi;
+}
+
+// The same search by one thread: galloping from lo, then bisection.
+__device__ __forceinline__ uint64_t thread_run_end(const uint32_t* __restrict__ col, uint64_t lo, uint64_t hi,
+                                                   uint32_t cb) {
+  if (lo >= hi || col[lo] >= cb) return lo;
+  uint64_t good = lo, step = 1;  // col[good] < cb
+  for (int i = 0; i < 64; ++i) {
+    const uint64_t p = good + step;
+    if (p >= hi) break;
+    if (col[p] >= cb) {
+      hi = p;
+      break;
+    }
+    good = p;
+    step <<= 1;
+  }
+  uint64_t a = good + 1, b = hi;
+  while (a < b) {
+    const uint64_t m = a + ((b - a) >> 1);
+    if (col[m] >= cb) b = m; else a = m + 1;
+  }
+  return a;
+}
+
+template <typename RP>
+__global__ void __launch_bounds__(kBitmapThreads, 1)
+    k_num_window(Csr<RP> A, Csr<RP> B, RowQueue q, OutSpec o, DevCounters* __restrict__ ctr,
+                 const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
+                 const uint64_t* __restrict__ bm_off, const unsigned long long* __restrict__ cache,
+                 unsigned long long* __restrict__ scratch, uint32_t* __restrict__ cursor,
+                 uint32_t* __restrict__ c_col, double* __restrict__ c_val) {
+  constexpr int NT = kBitmapThreads;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WinNumSmem& S = *reinterpret_cast<WinNumSmem*>(smem_raw);
+  double* vals = reinterpret_cast<double*>(S.area);
+  unsigned long long* wbits = S.area + kWinV;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < kWinV; i += NT) vals[i] = 0.0;
+  unsigned long long* my_scratch = scratch + (uint64_t)blockIdx.x * kBitmapWords;
+  const uint32_t count = *q.count;
+  const uint32_t stride = spread_stride(count);
+  for (;;) {
+    __syncthreads();  // every thread has read the previous row index
+    if (tid == 0) S.s_idx = atomicAdd(q.cursor, 1u);
+    __syncthreads();
+    const uint32_t idx = S.s_idx;
+    if (idx >= count) break;
+    const uint32_t row = q.rows[spread_index(idx, count, stride)];
+    const uint64_t rlo = lo[row], rhi = hi[row];
+    if (rhi - rlo + 1 > kBitmapBits) continue;  // wider rows: k_num_bitmap
+    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+    const uint64_t row_off = o.off[row];
+    const uint32_t expect = o.cap[row];
+    const uint32_t nw = (uint32_t)((rhi - rlo + 64) >> 6);
+    const uint64_t slot = cache ? bm_off[row] : ~0ull;
+    const unsigned long long* gbits;
+    if (slot != ~0ull) {
+      gbits = cache + slot;
+    } else {
+      // mark the row's bitmap over the slot area, keep a copy in this block's scratch
+      for (uint32_t w = tid; w < nw; w += NT) S.area[w] = 0ull;
+      __syncthreads();
+      block_for_each_product<NT, false>(A, B, a0, a1, S.e, [&](uint32_t c, double, bool ok) {
+        mark_bit(S.area, c, ok, true, rlo, rhi + 1);
+      });
+      for (uint32_t w = tid; w < nw; w += NT) my_scratch[w] = S.area[w];
+      __syncthreads();
+      for (int i = tid; i < kWinV; i += NT) vals[i] = 0.0;
+      __syncthreads();
+      gbits = my_scratch;
+    }
+    // resume cursors (offsets into each A entry's B row): registers when the
+    // row's A entries fit one chunk, else the per-entry array
+    const bool one_chunk = a1 - a0 <= (uint64_t)NT;
+    uint32_t my_cur = 0;
+    if (!one_chunk)
+      for (uint64_t k = a0 + tid; k < a1; k += NT) cursor[k] = 0u;
+    uint64_t r0 = 0;  // rank of the window's first entry within the row
+    for (uint32_t ws = 0; ws < nw;) {
+      const uint32_t wl = min(nw - ws, (uint32_t)kWinWords);
+      if (tid == 0) S.s_we = wl;
+      // window words and their popcounts, warp-major (warp w: words [256w, 256w + 256))
+      const uint32_t wbase = (uint32_t)warp * (kWinWords / 32);
+      uint32_t local = 0;
+#pragma unroll
+      for (int i = 0; i < kWinWords / 1024; ++i) {
+        const uint32_t w = wbase + 32u * i + lane;
+        const unsigned long long x = w < wl ? gbits[ws + w] : 0ull;
+        wbits[w] = x;
+        local += __popcll(x);
+      }
+#pragma unroll
+      for (int sh = 16; sh > 0; sh >>= 1) local += __shfl_xor_sync(kFull, local, sh);
+      uint32_t wtotal;
+      const uint32_t warp_base =
+          __shfl_sync(kFull, block_excl_scan<NT, uint32_t>(lane == 0 ? local : 0u, S.scan, &wtotal), 0);
+      uint32_t run = warp_base;
+#pragma unroll
+      for (int i = 0; i < kWinWords / 1024; ++i) {
+        const uint32_t w = wbase + 32u * i + lane;
+        const uint32_t pc = (uint32_t)__popcll(wbits[w]);
+        uint32_t x = pc;
+#pragma unroll
+        for (int sh = 1; sh < 32; sh <<= 1) {
+          const uint32_t y = __shfl_up_sync(kFull, x, sh);
+          if (lane >= sh) x += y;
+        }
+        const uint32_t ex = run + x - pc;
+        S.wpre[w] = (uint16_t)ex;  // exact below the window's end (<= kWinV)
+        // the word that takes the count past kWinV ends the window
+        if (w < wl && ex <= (uint32_t)kWinV && ex + pc > (uint32_t)kWinV) {
+          S.s_we = w;
+          S.s_nwin = ex;
+        }
+        run += __shfl_sync(kFull, x, 31);
+      }
+      __syncthreads();
+      const uint32_t we = S.s_we;
+      const uint32_t nwin = we == wl ? wtotal : S.s_nwin;
+      const uint64_t ca = rlo + 64ull * ws;
+      const uint32_t cb = (uint32_t)min((uint64_t)(rlo + 64ull * (ws + we)), (uint64_t)(rhi + 1));
+      // products whose column lies in [ca, cb), accumulated at their window rank
+      auto accumulate = [&](uint32_t c, double v, bool ok) {
+        if (ok) {
+          const uint32_t d = c - (uint32_t)ca;
+          const uint32_t w = d >> 6;
+          const uint32_t r = S.wpre[w] + (uint32_t)__popcll(wbits[w] & ((1ull << (d & 63)) - 1ull));
+          if (r < (uint32_t)kWinV) atomicAdd(&vals[r], v);
+        }
+      };
+      for (uint64_t c0 = a0; c0 < a1; c0 += NT) {
+        const uint32_t na = (uint32_t)min(a1 - c0, (uint64_t)NT);
+        const uint64_t k = c0 + tid;
+        unsigned long long bs = 0, be = 0, pos = 0;
+        double av = 0.0;
+        if (tid < (int)na) {
+          const uint32_t j = A.col[k];
+          bs = B.row_begin(j);
+          be = B.row_end(j);
+          pos = bs + (one_chunk ? my_cur : cursor[k]);
+          av = A.val[k];
+        }
+        unsigned long long end = pos;
+        if (na <= 64) {
+          // few entries: one warp searches each run
+          if (tid < (int)na) {
+            S.seg_pos[tid] = pos;
+            S.seg_end[tid] = be;
+          }
+          __syncthreads();
+          for (uint32_t e = warp; e < na; e += NT / 32) {
+            const uint64_t r = warp_run_end(B.col, S.seg_pos[e], S.seg_end[e], cb);
+            __syncwarp();
+            if (lane == 0) S.seg_end[e] = r;
+          }
+          __syncthreads();
+          if (tid < (int)na) end = S.seg_end[tid];
+        } else if (tid < (int)na) {
+          end = thread_run_end(B.col, pos, be, cb);
+        }
+        if (tid < (int)na) {
+          if (one_chunk) my_cur = (uint32_t)(end - bs);
+          else cursor[k] = (uint32_t)(end - bs);
+        }
+        block_pack_chunk<NT, true>(pos, end - pos, av, S.e);
+        block_run_chunk<NT, true>(B, S.e, accumulate);
+      }
+      // the window's entries in rank order: column ids from the bitmap, values
+      // from the slots (which are cleared for the next window)
+      const uint64_t wout = row_off + r0;
+      const uint64_t row_lim = row_off + expect;
+      for (uint32_t wb = (uint32_t)warp * 32u; wb < we; wb += 32u * (NT / 32)) {
+        const uint32_t w = wb + lane;
+        const uint32_t gpre = S.wpre[wb];
+        const uint64_t gcol = ca + (uint64_t)wb * 64;
+        warp_emit_group(w < we ? wbits[w] : 0ull, lane, [&](uint32_t j, uint32_t b) {
+          const uint32_t lr = gpre + j;
+          const uint64_t at = wout + lr;
+          const double v = vals[lr];
+          vals[lr] = 0.0;
+          if (at < row_lim) {
+            c_col[at] = (uint32_t)(gcol + b);
+            c_val[at] = v;
+          }
+        });
+      }
+      __syncthreads();
+      r0 += nwin;
+      ws += we;
+    }
+    if (tid == 0 && r0 != expect) raise_status(ctr, DEV_COUNT_MISMATCH, row);
   }
 }
 
@@ -1337,6 +1624,7 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
       const NumPolicy& pol = pols.p[row_pol ? row_pol[i] : 0];
       b = num_bin_for(v[q], p, (uint64_t)hi[i] - lo[i] + 1, pol);
       if (b >= 0 && pol.force_bin < 0 && bm_off[i] != ~0ull) b = NB_BITMAP;  // reuse the saved bitmap
+      if (b == NB_BITMAP && (uint64_t)hi[i] - lo[i] + 1 > kBitmapBits) atomicAdd(&ctr->num_wide, 1u);
 #pragma unroll
       for (int c = 0; c < NB_COUNT; ++c) {
         if (b == c) {
@@ -1562,6 +1850,7 @@ __global__ void __launch_bounds__(256) k_row_bounds(uint64_t rows, const uint32_
 // ---------------------------------------------------------------- launchers
 namespace {
 constexpr size_t kNumBitmapSmem = sizeof(BitmapNumSmem);
+constexpr size_t kWinNumSmem = sizeof(WinNumSmem);
 constexpr size_t kSymBitmapSmem = sizeof(BitmapSymSmem);
 template <int NT, int LOG2T>
 constexpr size_t num_hash_smem() { return sizeof(NumHashSmem<NT, LOG2T>); }
@@ -1570,7 +1859,7 @@ constexpr size_t sym_hash_smem() { return sizeof(SymHashSmem<NT, LOG2T>); }
 
 int g_occ[24];  // resident blocks per SM of each persistent kernel (same order as kinds)
 enum Kind { K_SYM_ESC1, K_SYM_ESC2, K_SYM_ESC4, K_SYM_S, K_SYM_M, K_SYM_L, K_SYM_BM,
-            K_NUM_ESC1, K_NUM_ESC2, K_NUM_ESC4, K_NUM_S, K_NUM_M, K_NUM_L, K_NUM_BM };
+            K_NUM_ESC1, K_NUM_ESC2, K_NUM_ESC4, K_NUM_S, K_NUM_M, K_NUM_L, K_NUM_BM, K_NUM_WIN };
 
 template <typename F>
 int occ_of(F f, int threads, size_t smem) {
@@ -1588,6 +1877,7 @@ template <typename RP>
 void set_attrs() {
   allow_smem(k_sym_bitmap<RP>, kSymBitmapSmem);
   allow_smem(k_num_bitmap<RP>, kNumBitmapSmem);
+  allow_smem(k_num_window<RP>, kWinNumSmem);
   allow_smem(k_sym_hash<RP, 128, 11>, sym_hash_smem<128, 11>());
   allow_smem(k_sym_hash<RP, 256, 13>, sym_hash_smem<256, 13>());
   allow_smem(k_sym_hash<RP, 512, 15>, sym_hash_smem<512, 15>());
@@ -1614,7 +1904,25 @@ void configure_kernel_attributes() {
   g_occ[K_NUM_M] = occ_of(k_num_hash<uint32_t, 256, 12>, 256, num_hash_smem<256, 12>());
   g_occ[K_NUM_L] = occ_of(k_num_hash<uint32_t, 512, 13>, 512, num_hash_smem<512, 13>());
   g_occ[K_NUM_BM] = occ_of(k_num_bitmap<uint32_t>, kBitmapThreads, kNumBitmapSmem);
+  g_occ[K_NUM_WIN] = occ_of(k_num_window<uint32_t>, kBitmapThreads, kWinNumSmem);
 }
+
+namespace {
+std::mutex g_attr_mutex;
+bool g_attr_done[64] = {false};
+}  // namespace
+
+bool ensure_kernel_attributes(int dev) {
+  std::lock_guard<std::mutex> lock(g_attr_mutex);
+  if (dev < 0 || dev >= 64) return false;
+  if (!g_attr_done[dev]) {
+    configure_kernel_attributes();
+    g_attr_done[dev] = true;
+  }
+  return true;
+}
+
+size_t window_scratch_words(int num_sms) { return (size_t)num_sms * (size_t)g_occ[K_NUM_WIN] * kBitmapWords; }
 
 template <typename RP>
 int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const SymPolicy& pol,
@@ -1742,9 +2050,24 @@ int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const O
     k_num_hash<RP, 512, 13><<<gsz, 512, num_hash_smem<512, 13>(), s>>>(A, B, queue(NB_HASH_L), o, w.ctr, w.prod,
                                                                        w.lo, w.hi, c_col, c_val);
   mark(NB_BITMAP);
-  if ((gsz = grid(K_NUM_BM, NB_BITMAP, 1)) && ++launched)
+  const bool windowed = !o.count && w.win_cursor && w.win_scratch;
+  if (windowed) {
+    // rows up to 2^20 columns wide in the windowed kernel, wider ones in
+    // k_num_bitmap (own queue cursor), launched only when there are any
+    if ((gsz = grid(K_NUM_WIN, NB_BITMAP, 1)) && ++launched)
+      k_num_window<RP><<<gsz, kBitmapThreads, kWinNumSmem, s>>>(A, B, queue(NB_BITMAP), o, w.ctr, w.lo, w.hi,
+                                                                w.bm_off, w.bm_cache, w.win_scratch, w.win_cursor,
+                                                                c_col, c_val);
+    if (w.wide_rows && (gsz = grid(K_NUM_BM, NB_BITMAP, 1)) && ++launched) {
+      const RowQueue wq{w.num_bins + (uint64_t)NB_BITMAP * A.rows, w.ctr->num_count + NB_BITMAP,
+                        &w.ctr->wide_cursor};
+      k_num_bitmap<RP><<<gsz, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, wq, o, w.ctr, w.prod, w.lo, w.hi,
+                                                                   w.bm_off, w.bm_cache, c_col, c_val, true);
+    }
+  } else if ((gsz = grid(K_NUM_BM, NB_BITMAP, 1)) && ++launched) {
     k_num_bitmap<RP><<<gsz, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, queue(NB_BITMAP), o, w.ctr, w.prod, w.lo,
-                                                                 w.hi, w.bm_off, w.bm_cache, c_col, c_val);
+                                                                 w.hi, w.bm_off, w.bm_cache, c_col, c_val, false);
+  }
   mark(NB_COUNT);
   return launched;
 }
@@ -1808,7 +2131,7 @@ int launch_overflow(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, bool n
   } else {
     const OutSpec o{w.rowptr64, w.cnt, nullptr, nullptr, nullptr};
     k_num_bitmap<RP><<<num_sms, kBitmapThreads, kNumBitmapSmem, s>>>(A, B, q, o, w.ctr, w.prod, w.lo, w.hi, w.bm_off,
-                                                                     nullptr, c_col, c_val);
+                                                                     nullptr, c_col, c_val, false);
   }
   return 1;
 }

@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <fstream>
 #include <memory>
 #include <sstream>
@@ -89,6 +90,7 @@ struct Stats {
   uint64_t sym_prod[SB_COUNT] = {0};
   uint64_t cache_words = 0, cache_used = 0;
   bool cache_dropped = false;
+  int bm_kernel = 0;  // numeric bitmap class: 0 no rows, 1 k_num_bitmap (rank + FP64 red), 2 k_num_window
   int launches = 0;  // kernels launched by the last call
   uint64_t total_est = 0, overflow_rows = 0;
   int hll_log2p = 0;
@@ -195,6 +197,11 @@ struct ocean_handle {
   // saved row bitmaps of the symbolic pass (grow-only, kept across calls)
   unsigned long long* cache_buf = nullptr;
   uint64_t cache_cap_words = 0;
+  // k_num_window: resume cursors per A entry and per-block bitmaps (grow-only)
+  uint32_t* win_cursor = nullptr;
+  uint64_t win_cursor_cap = 0;
+  unsigned long long* win_scratch = nullptr;
+  uint64_t win_scratch_cap = 0;
 
   void free_all() {
     DevWork& x = w;
@@ -207,6 +214,8 @@ struct ocean_handle {
     if (out_col) cudaFreeHost(out_col);
     if (out_val) cudaFreeHost(out_val);
     if (cache_buf) cudaFree(cache_buf);
+    if (win_cursor) cudaFree(win_cursor);
+    if (win_scratch) cudaFree(win_scratch);
     if (mlp_dev) cudaFree(mlp_dev);
     if (raw_est) cudaFree(raw_est);
     if (row_pol) cudaFree(row_pol);
@@ -228,13 +237,17 @@ void init_handle(ocean_handle* h, const std::string& json) {
   OCEAN_CUDA(cudaDeviceGetDefaultMemPool(&pool, h->device));
   uint64_t threshold = UINT64_MAX;
   OCEAN_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
-  static bool configured[64] = {false};
-  if (h->device < 64 && !configured[h->device]) {
-    configure_kernel_attributes();
-    configure_mlp_attributes();
-    OCEAN_CUDA(cudaGetLastError());
-    configured[h->device] = true;
+  static std::mutex mlp_mutex;
+  static bool mlp_configured[64] = {false};
+  OCEAN_CHECK(ensure_kernel_attributes(h->device), OCEAN_ERR_INVALID, "device ordinal out of range (64 devices)");
+  {
+    std::lock_guard<std::mutex> lock(mlp_mutex);
+    if (!mlp_configured[h->device]) {
+      configure_mlp_attributes();
+      mlp_configured[h->device] = true;
+    }
   }
+  OCEAN_CUDA(cudaGetLastError());
   for (auto& e : h->ev) OCEAN_CUDA(cudaEventCreate(&e));
   OCEAN_CUDA(cudaHostAlloc((void**)&h->h_ctr, sizeof(DevCounters), cudaHostAllocDefault));
   OCEAN_CUDA(cudaMalloc((void**)&h->w.ctr, sizeof(DevCounters)));
@@ -498,6 +511,38 @@ void dispatch_segments(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cuda
     OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
     OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
   }
+}
+
+// Buffers of the windowed exact numeric kernel for the bitmap class: cursors
+// for nnz(A) entries when a row of A has more than one chunk (1024) of
+// entries, and one 2^20-bit bitmap per resident block. If they cannot be
+// allocated, the class runs in k_num_bitmap alone (no error).
+void prepare_windows(ocean_handle* h, uint64_t a_nnz, unsigned bitmap_rows) {
+  h->w.win_cursor = nullptr;
+  h->w.win_scratch = nullptr;
+  h->w.wide_rows = h->h_ctr->num_wide;
+  h->st.bm_kernel = bitmap_rows ? 1 : 0;
+  if (!h->cfg.numeric_windows || bitmap_rows == 0) return;
+  const uint64_t need_cur = h->h_ctr->max_a_nnz > (unsigned)kBitmapThreads ? a_nnz : 1;
+  const uint64_t need_scr = window_scratch_words(h->num_sms);
+  auto try_grow = [](auto*& p, uint64_t& cap, uint64_t need, size_t elem) {
+    if (p && cap >= need) return true;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc((void**)&p, need * elem) != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return false;
+    }
+    cap = need;
+    return true;
+  };
+  if (!try_grow(h->win_cursor, h->win_cursor_cap, need_cur, sizeof(uint32_t))) return;
+  if (!try_grow(h->win_scratch, h->win_scratch_cap, need_scr, sizeof(unsigned long long))) return;
+  h->w.win_cursor = h->win_cursor;
+  h->w.win_scratch = h->win_scratch;
+  h->st.bm_kernel = 2;
 }
 
 // Phase 2 of the precise workflow: symbolic class kernels (exact counts into
@@ -859,6 +904,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         unsigned num_counts[NB_COUNT];
         for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
         const OutSpec est_out{h->w.est_off, h->w.est, h->w.cnt, h->w.ovf, &h->w.ctr->overflow_n};
+        st.bm_kernel = num_counts[NB_BITMAP] ? 1 : 0;
         st.launches += launch_numeric(A, B, h->w, est_out, (uint32_t*)t_col, (double*)t_val, h->num_sms, s,
                                       track ? h->ev + EV_NUM0 : nullptr, class_counts ? num_counts : nullptr);
         if (track) h->ev_mask |= ((1ull << (NB_COUNT + 1)) - 1) << EV_NUM0;
@@ -889,6 +935,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
       if (wf == WF_PRECISE) {
         unsigned num_counts[NB_COUNT];
         for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
+        prepare_windows(h, A.nnz, num_counts[NB_BITMAP]);
         const OutSpec exact{h->w.rowptr64, h->w.row_nnz, nullptr, nullptr, nullptr};
         st.launches += launch_numeric(A, B, h->w, exact, owner->col, owner->val, h->num_sms, s,
                                       track ? h->ev + EV_NUM0 : nullptr, num_counts);
@@ -1021,7 +1068,8 @@ std::string stats_json(ocean_handle* h) {
   o << "\"decision\": {\"workflow\": " << st.workflow << ", \"rowptr_bits\": " << st.rowptr_bits
     << ", \"bitmap_cache_bytes\": " << 8 * st.cache_words << ", \"bitmap_cache_used_bytes\": " << 8 * st.cache_used
     << ", \"bitmap_cache_dropped\": " << (st.cache_dropped ? "true" : "false")
-    << ", \"kernel_launches\": " << st.launches << "}, ";
+    << ", \"numeric_bitmap_kernel\": \"" << (st.bm_kernel == 2 ? "window" : st.bm_kernel == 1 ? "rank" : "none")
+    << "\", \"kernel_launches\": " << st.launches << "}, ";
   if (st.sampled)
     o << "\"sampling\": {\"compaction_1\": " << st.compaction1 << ", \"compaction_2\": " << st.compaction2
       << "}, ";

@@ -67,7 +67,9 @@ struct DevCounters {
   double sample_compaction;               // HLL sampling: sum of products / estimate over samples
   unsigned int status;     // OR of DevError bits
   unsigned int err_row;
-  unsigned int pad[4];
+  unsigned int num_wide;     // numeric bitmap-class rows whose column span exceeds one 2^20-bit bitmap
+  unsigned int wide_cursor;  // queue cursor of those rows' kernel (k_num_bitmap beside k_num_window)
+  unsigned int pad[2];
 };
 
 enum DevError : unsigned int {

@@ -20,13 +20,17 @@
 //
 // Set-up: the first call on a device, with that device current, resolves the
 // array's device address with cudaGetSymbolAddress and sets the kernels'
-// shared-memory limits; make that first call before any stream capture.
+// shared-memory limits; make that first call before any stream capture. The
+// address is kept for the life of the process: a cudaDeviceReset after the
+// first call is not supported (the module, and with it the array, is reloaded
+// at another address).
 // All calls share the one array and it keeps the last call's contents: each
 // call clears the counters it relies on (a stream-ordered memset), and calls
 // that overlap on the GPU (different streams, no ordering between them) race on
 // the array, so callers must order them (one stream, or events).
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdio>
 #include <mutex>
 
@@ -69,7 +73,10 @@ bool setup_device(int dev, void** addr, int* sms, char* err, size_t errlen) {
       snprintf(err, errlen, "cudaDeviceGetAttribute: %s", cudaGetErrorString(e2));
       return false;
     }
-    configure_kernel_attributes();
+    if (!ensure_kernel_attributes(dev)) {
+      snprintf(err, errlen, "device ordinal %d out of range", dev);
+      return false;
+    }
     g_num_sms[dev] = n;
     g_scratch_addr[dev] = p;
   }
@@ -115,15 +122,23 @@ int run_noalloc(const ocean_csr_view* A, const ocean_csr_view* B, uint32_t* row_
     launch_symbolic(a, b, w, sms, s, nullptr, nullptr);
     e = cudaGetLastError();
   }
-  unsigned status = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &w.ctr->status, sizeof(status), cudaMemcpyDeviceToHost, s);
+  // status and err_row are adjacent in the counters: one read-back of both
+  static_assert(offsetof(DevCounters, err_row) == offsetof(DevCounters, status) + sizeof(unsigned),
+                "status and err_row must be adjacent");
+  unsigned st[2] = {0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(st, &w.ctr->status, sizeof(st), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     set_last_error(cudaGetErrorString(e));
     return OCEAN_ERR_CUDA;
   }
-  if (status) {
-    set_last_error("a row exceeded the capacity of its accumulator class");
+  if (st[0]) {
+    char msg[256];
+    const char* what = (st[0] & DEV_TABLE_FULL)     ? "a shared-memory hash table ran full (probe limit reached)"
+                       : (st[0] & DEV_BIN_OVERFLOW) ? "a row exceeded the capacity of its accumulator class"
+                                                    : "device error";
+    snprintf(msg, sizeof msg, "ocean_symbolic_noalloc: %s (status 0x%x, first row %u)", what, st[0], st[1]);
+    set_last_error(msg);
     return OCEAN_ERR_CAPACITY;
   }
   return OCEAN_OK;

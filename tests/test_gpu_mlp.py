@@ -62,9 +62,13 @@ def test_gradient_matches_oracle(n):
     want, loss = N.grad(p, mu, isd, f, t, float(n))
     blocks = {"W1": (N.OFF_W1, N.OFF_B1), "b1": (N.OFF_B1, N.OFF_W2), "W2": (N.OFF_W2, N.OFF_B2),
               "b2": (N.OFF_B2, N.OFF_W3), "w3": (N.OFF_W3, N.OFF_B3), "b3": (N.OFF_B3, N.P)}
+    # the oracle rounds the activations and operands to BF16 where the kernels
+    # do, so only accumulation order (and a rare flipped BF16 rounding) differs
+    rels = {}
     for name, (a, b) in blocks.items():
-        rel = np.linalg.norm(got[a:b] - want[a:b]) / max(np.linalg.norm(want[a:b]), 1e-12)
-        assert rel < 2e-2, (name, rel)
+        rels[name] = float(np.linalg.norm(got[a:b] - want[a:b]) / max(np.linalg.norm(want[a:b]), 1e-12))
+    print("gradient relative error per block:", rels)
+    assert all(r < 5e-3 for r in rels.values()), rels
     assert abs(float(lbuf.item()) - loss) <= 1e-3 * loss
 
 

@@ -4,7 +4,10 @@ application arena or caching allocator) or may not call cudaMalloc in steady
 state. Its scratch is a fixed device array inside the library, so it checks:
   * two calls in a row through the C ABI (a different matrix each time, so the
     second call must not see the first call's scratch contents) give exactly
-    the counts of the regular entry point ocean_symbolic;
+    the counts of the regular entry point ocean_symbolic and of the CPU oracle,
+    with 32- and with 64-bit row pointers;
+  * a call after a warm-up call leaves the device's free memory and torch's
+    allocated bytes unchanged (nothing is allocated on this path);
   * an A with more rows than the fixed scratch allows is refused with
     OCEAN_ERR_INVALID.
 This file is collected last on purpose (name order)."""
@@ -13,6 +16,7 @@ import ctypes
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from research_b200 import matrices as M
 from research_b200.ocean import CsrView, DeviceCSR, SpGEMM, lib
 
@@ -30,17 +34,38 @@ def noalloc_counts(dA, dB):
     return out.cpu().numpy().view(np.uint32)
 
 
-def test_noalloc_matches_regular_entry_point_twice():
+@pytest.mark.parametrize("bits", [32, 64])
+def test_noalloc_matches_regular_entry_point_twice(bits):
     # first a skewed R-MAT (every class, bitmap rows included), then a smaller
     # uniform matrix: the second call reuses the scratch the first one filled
     cases = [M.rmat(17, 16, seed=31), M.uniform_random(40000, 12, seed=32)]
     g = SpGEMM()
     for A in cases:
+        if bits == 64:
+            A = A.widened()
         dA = DeviceCSR.from_host(A)
         got = noalloc_counts(dA, dA)
         want = g.symbolic(dA, dA).cpu().numpy().view(np.uint32)
         assert got.shape == want.shape
         assert np.array_equal(got, want)
+        assert np.array_equal(got, O.symbolic(A, A).astype(np.uint32))
+
+
+def test_noalloc_call_allocates_nothing():
+    import torch
+    A = M.rmat(16, 16, seed=34)
+    dA = DeviceCSR.from_host(A)
+    out = torch.empty(A.rows, dtype=torch.int32, device="cuda")
+    av = dA.view()
+    assert lib().ocean_symbolic_noalloc(ctypes.byref(av), ctypes.byref(av), out.data_ptr(), None) == 0  # warm-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    assert lib().ocean_symbolic_noalloc(ctypes.byref(av), ctypes.byref(av), out.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
 
 
 def test_noalloc_rejects_more_rows_than_scratch():
