@@ -812,6 +812,15 @@ def leg_batch(stream, steps: int = 3, warmup: int = 2, e2e_steps: int = 2, ablat
         out[name] = rec
         plan.close()
         gb.close()
+        if name == "learned_batched" and e2e_steps > 0:
+            # the same batch as 8 plans of 64 problems with the tuned policy,
+            # pipelined over three streams: inputs of plan i+1 copied in and
+            # plan i computed while plan i-1's results are copied back
+            tuned = {k: info[k] for k in ("esc_max_products", "hash_s_max_scale", "bitmap_words_scale") if k in info}
+            pe = batch_e2e_pipelined(dA, {"use_learned_estimator": True, **tuned}, stream, e2e_steps, chunks=8)
+            pe["gflops"] = gf(pe["ms"])
+            rec["e2e_pipelined"] = pe
+            rec["e2e_pipelined_speedup_vs_plain"] = round(out["plain"]["e2e_ms"] / pe["ms"], 3)
     gp.close()
     return out
 
@@ -854,6 +863,69 @@ def batch_e2e(plan, info, dA, gp, stream, steps: int) -> dict:
             "d2h_bytes_per_step": int(rp_out.nbytes + 12 * nnz_c),
             "api": "pinned host inputs -> device, ocean_batch_launch, ocean_batch_download; "
                    "plain: 512 x ocean_spgemm_host"}
+
+
+def batch_e2e_pipelined(dA, config: dict, stream, steps: int, chunks: int = 8) -> dict:
+    """End-to-end ms of one step of the batch as `chunks` captured plans on
+    three streams (copy in, compute, copy out; ocean_batch_launch and
+    ocean_batch_download_async), CUDA events on `stream` around the step."""
+    import torch
+    from research_b200.ocean import Batch, SpGEMM
+    n = len(dA)
+    bounds = [round(i * n / chunks) for i in range(chunks + 1)]
+    g = SpGEMM(config)
+    plans, parts = [], []
+    for i in range(chunks):
+        part = dA[bounds[i]:bounds[i + 1]]
+        plans.append(Batch(g, part, stream=stream.cuda_stream))
+        parts.append(part)
+    infos = [pl.info() for pl in plans]
+
+    def pinned_like(t):
+        return torch.empty(t.shape, dtype=t.dtype, pin_memory=True).copy_(t.cpu())
+    hosts = [[(pinned_like(a.rowptr), pinned_like(a.col), pinned_like(a.val)) for a in part] for part in parts]
+    outs = []
+    for inf in infos:
+        wide = inf["rowptr_bits"] == 64
+        outs.append((torch.empty(int(inf["rows"]) + int(inf["problems"]), dtype=torch.int64 if wide else torch.int32,
+                                 pin_memory=True),
+                     torch.empty(max(int(inf["nnz_c"]), 1), dtype=torch.int32, pin_memory=True),
+                     torch.empty(max(int(inf["nnz_c"]), 1), dtype=torch.float64, pin_memory=True)))
+    s_in, s_comp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+
+    def step():
+        start = torch.cuda.Event()
+        start.record(stream)
+        for st in (s_in, s_comp, s_out):
+            st.wait_event(start)
+        done = None
+        for pl, part, hs, (rp, col, val) in zip(plans, parts, hosts, outs):
+            with torch.cuda.stream(s_in):
+                for a, (r, c, v) in zip(part, hs):
+                    a.rowptr.copy_(r, non_blocking=True)
+                    a.col.copy_(c, non_blocking=True)
+                    a.val.copy_(v, non_blocking=True)
+            e_in = torch.cuda.Event()
+            e_in.record(s_in)
+            s_comp.wait_event(e_in)
+            pl.launch(s_comp.cuda_stream)
+            e_c = torch.cuda.Event()
+            e_c.record(s_comp)
+            s_out.wait_event(e_c)
+            pl.download_into(rp.numpy(), col.numpy(), val.numpy(), s_out.cuda_stream, wait=False)
+            done = torch.cuda.Event()
+            done.record(s_out)
+        stream.wait_event(done)
+    ms = time_on_device(step, steps, 1, stream)
+    res = {"ms": round(ms, 3), "chunks": chunks, "kernel_launches_per_plan": infos[0]["kernel_launches"],
+           "h2d_bytes_per_step": int(sum(x.nbytes for hs in hosts for h in hs for x in h)),
+           "d2h_bytes_per_step": int(sum(o[0].nbytes + 12 * int(inf["nnz_c"]) for o, inf in zip(outs, infos))),
+           "api": "8 x (ocean_batch_create once; per step ocean_batch_launch, ocean_batch_download_async) "
+                  "on copy-in/compute/copy-out streams"}
+    for pl in plans:
+        pl.close()
+    g.close()
+    return res
 
 
 def extra_legs(args, stream) -> dict:

@@ -222,6 +222,11 @@ int ocean_batch_results(ocean_batch* b, ocean_csr* C);
  * values each, of the width in the results' rowptr_bits), col and val the
  * problems' entries one after another (the sum of their nnz). */
 int ocean_batch_download(ocean_batch* b, void* rowptrs, uint32_t* col, double* val, void* stream);
+/* The same copies, queued on `stream` without waiting, so that a pipeline of
+ * several plans can copy one plan's results back while another computes (the
+ * host buffers should be pinned; the caller synchronizes the stream). No
+ * counterpart in the reference. */
+int ocean_batch_download_async(ocean_batch* b, void* rowptrs, uint32_t* col, double* val, void* stream);
 /* Plan facts as JSON: sizes, workflow, estimator, kernels per run, tuned policy. */
 int ocean_batch_info_json(ocean_batch* b, char* buf, size_t cap, size_t* needed);
 int ocean_batch_destroy(ocean_batch* b);

@@ -200,7 +200,9 @@ struct Config {
   double bitmap_words_scale = 1.0;      // > 0: scales the column-span limits under which mid rows use bitmaps
   bool prefer_direct_hash = true;       // mid rows whose column span fits a hash table use it (direct slots)
   bool numeric_windows = false;         // exact numeric bitmap class: shared-memory value windows (k_num_window)
+  bool fused_ultrasparse = false;       // ultra-sparse inputs (<= 256 products per row): one fused launch
   bool batch_autotune = false;          // batched plans: search the class policy on the batch before capturing
+  std::string autotune_cache_file;      // JSON-lines cache of tuned policies (key: GPU name + batch features); "" off
   // segment-driven dispatch: rows of each spy-plot segment class take that
   // class's policy (index = SegClass: sparse_uniform, dense, power_law, banded);
   // unset fields inherit the global policy above
@@ -285,7 +287,9 @@ struct Config {
     getd("bitmap_words_scale", c.bitmap_words_scale);
     getb("prefer_direct_hash", c.prefer_direct_hash);
     getb("numeric_windows", c.numeric_windows);
+    getb("fused_ultrasparse", c.fused_ultrasparse);
     getb("batch_autotune", c.batch_autotune);
+    gets("autotune_cache_file", c.autotune_cache_file);
     getb("use_segment_dispatch", c.use_segment_dispatch);
     static const char* kSegKey[4] = {"sparse_uniform", "dense", "power_law", "banded"};
     for (int k = 0; k < 4; ++k) {

@@ -156,6 +156,16 @@ int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const O
 
 void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, cudaStream_t s);
 
+// Fused ultra-sparse multiply (every row at most 256 products): C's column
+// ids and values (capacity `cap` >= the sum of the products) and the row
+// pointers w.rowptr64 (and w.rowptr32 when rowptr32) in one launch, nnz(C) into
+// w.ctr->total_nnz. `tiles` holds usp_tiles(A.rows) words.
+template <typename RP>
+int launch_usp_fused(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, unsigned long long* tiles, uint64_t cap,
+                     bool rowptr32, uint32_t* c_col, double* c_val, cudaStream_t s);
+uint64_t usp_tiles(uint64_t rows);
+constexpr uint32_t kUspMaxProducts = 256;
+
 // out[r] = min(products, column span) for every row of the last analysis.
 int launch_row_bounds(const DevWork& w, uint32_t* out, cudaStream_t s);
 

@@ -486,6 +486,286 @@ __global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, RowQueue 
   }
 }
 
+// ---------------------------------------------------------------- fused ultra-sparse multiply
+// One launch for an input whose every row has at most 256 products (the
+// ultra-sparse workflow's inputs): each warp merges one row of C in registers
+// (the ESC classes' register sort and segmented sums; rows of 129-256 products
+// sort one packed 64-bit key per product in shared memory first) and stages
+// it in shared memory; a block's 8 rows form a tile whose output offset comes
+// from a decoupled look-back over the preceding tiles' published counts
+// (tile ids are taken in launch order, so every tile waits only on tiles that
+// already run); then the rows are written at their final place in C and the
+// row pointers with them. No temporary output, no separate scan, no copy.
+// The look-back's wait is bounded: after kUspSpinLimit polls the block flags
+// DEV_SCAN_TIMEOUT and continues with a smaller prefix, which keeps every
+// write inside C's capacity (the sum of the products).
+constexpr int kUspWarps = 8;     // rows per tile, one per warp
+constexpr int kUspCap = 256;     // products per row
+constexpr unsigned long long kTileAgg = 1ull << 62, kTileIncl = 2ull << 62, kTileVal = (1ull << 62) - 1;
+constexpr int kUspSpinLimit = 1 << 20;
+
+struct UspSmem {
+  uint64_t src[kUspWarps][kUspCap];   // gathered B indices; packed sort keys of the largest rows
+  uint64_t aidx[kUspWarps][kUspCap];  // gathered A indices
+  uint32_t okey[kUspWarps][kUspCap];  // merged row: column ids
+  double oval[kUspWarps][kUspCap];    // merged row: values (scratch of the packed sorts before)
+  uint32_t cnt[kUspWarps];
+  uint32_t np[kUspWarps];
+  unsigned long long prefix;
+  uint32_t tile;
+};
+
+// Segmented sums of the sorted (key, val) of one row (kEmpty keys last), then
+// the distinct columns and their sums written compactly to okey/oval.
+// Returns the row's output count. Warp-collective.
+template <int K>
+__device__ __forceinline__ uint32_t usp_merge_stage(uint32_t (&key)[K], double (&val)[K], uint32_t* okey,
+                                                    double* oval) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int e = 0; e < K; ++e) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t ck = __shfl_down_sync(kFull, key[e], d);
+      const double cv = __shfl_down_sync(kFull, val[e], d);
+      if (lane + d < 32 && ck == key[e]) val[e] += cv;
+    }
+  }
+  uint32_t carry_key = kEmpty;
+  double carry = 0.0;
+#pragma unroll
+  for (int e = K - 1; e >= 0; --e) {
+    const uint32_t last = __shfl_sync(kFull, key[e], 31);
+    if (key[e] == last && last == carry_key && last != kEmpty) val[e] += carry;
+    carry_key = __shfl_sync(kFull, key[e], 0);
+    carry = __shfl_sync(kFull, val[e], 0);
+  }
+  unsigned hb[K];
+  bool head[K];
+  warp_run_heads<K>(key, hb, head);
+  uint32_t before = 0;
+#pragma unroll
+  for (int e = 0; e < K; ++e) {
+    if (head[e]) {
+      const uint32_t pos = before + __popc(hb[e] & lanemask_lt());
+      okey[pos] = key[e];
+      oval[pos] = val[e];
+    }
+    before += __popc(hb[e]);
+  }
+  __syncwarp();
+  return before;
+}
+
+// Register ESC of a row of np <= 32K products gathered in src/aidx; the
+// merged row goes to okey/oval. Returns the output count.
+template <int K, typename RP>
+__device__ __forceinline__ uint32_t usp_row_regs(const Csr<RP>& A, const Csr<RP>& B, uint32_t np,
+                                                 const uint64_t* src, const uint64_t* aidx, uint32_t* okey,
+                                                 double* oval) {
+  constexpr int LOGN = K == 1 ? 5 : (K == 2 ? 6 : 7);
+  const int lane = threadIdx.x & 31;
+  uint32_t key[K];
+  double val[K];
+#pragma unroll
+  for (int e = 0; e < K; ++e) {
+    const uint32_t i = (uint32_t)(e << 5) | lane;
+    key[e] = kEmpty;
+    val[e] = 0.0;
+    if (i < np) {
+      const uint64_t sidx = src[i];
+      key[e] = B.col[sidx];
+      val[e] = A.val[aidx[i]] * B.val[sidx];
+    }
+  }
+  uint32_t kmin = kEmpty, kmax = 0;
+#pragma unroll
+  for (int e = 0; e < K; ++e) {
+    kmin = min(kmin, key[e]);
+    if (key[e] != kEmpty) kmax = max(kmax, key[e]);
+  }
+  kmin = __reduce_min_sync(kFull, kmin);
+  kmax = __reduce_max_sync(kFull, kmax);
+  if (kmin == kEmpty || kmax - kmin < (1u << (32 - LOGN)) - 1u) {
+    uint32_t pk[K];
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+      const uint32_t pos = (uint32_t)(e << 5) | lane;
+      oval[pos] = val[e];
+      pk[e] = key[e] == kEmpty ? kEmpty : ((key[e] - kmin) << LOGN) | pos;
+    }
+    __syncwarp();
+    warp_bitonic_sort<K, false>(pk, val);
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+      if (pk[e] == kEmpty) {
+        key[e] = kEmpty;
+        val[e] = 0.0;
+      } else {
+        key[e] = (pk[e] >> LOGN) + kmin;
+        val[e] = oval[pk[e] & (32 * K - 1)];
+      }
+    }
+    __syncwarp();
+  } else {
+    warp_bitonic_sort<K, true>(key, val);
+  }
+  return usp_merge_stage<K>(key, val, okey, oval);
+}
+
+// A row of 129-256 products: one 64-bit key (column << 8 | position) per
+// product bitonic-sorted in shared memory, then merged in registers.
+template <typename RP>
+__device__ __forceinline__ uint32_t usp_row_smem(const Csr<RP>& A, const Csr<RP>& B, uint32_t np, uint64_t* src,
+                                                 const uint64_t* aidx, uint32_t* okey, double* oval) {
+  const int lane = threadIdx.x & 31;
+  for (uint32_t i = lane; i < (uint32_t)kUspCap; i += 32) {
+    uint64_t kk = ~0ull;
+    if (i < np) {
+      const uint64_t sidx = src[i];
+      kk = ((uint64_t)B.col[sidx] << 8) | i;
+      oval[i] = A.val[aidx[i]] * B.val[sidx];
+    }
+    src[i] = kk;
+  }
+  __syncwarp();
+  for (int k = 2; k <= kUspCap; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = lane; t < kUspCap / 2; t += 32) {
+        const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+        const int l = i + j;
+        const bool asc = (i & k) == 0;
+        const uint64_t a = src[i], b = src[l];
+        if ((a > b) == asc) {
+          src[i] = b;
+          src[l] = a;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  uint32_t key[8];
+  double val[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const uint64_t kk = src[(e << 5) | lane];
+    key[e] = kk == ~0ull ? kEmpty : (uint32_t)(kk >> 8);
+    val[e] = kk == ~0ull ? 0.0 : oval[kk & 255];
+  }
+  __syncwarp();
+  return usp_merge_stage<8>(key, val, okey, oval);
+}
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+
+template <typename RP>
+__global__ void __launch_bounds__(256) k_usp_fused(Csr<RP> A, Csr<RP> B, unsigned long long* __restrict__ tiles,
+                                                   DevCounters* __restrict__ ctr, uint64_t cap,
+                                                   uint64_t* __restrict__ rowptr64, uint32_t* __restrict__ rowptr32,
+                                                   uint32_t* __restrict__ c_col, double* __restrict__ c_val) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  UspSmem& S = *reinterpret_cast<UspSmem*>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) S.tile = atomicAdd(&ctr->usp_tile, 1u);
+  __syncthreads();
+  const uint32_t t = S.tile;
+  const uint64_t row = (uint64_t)t * kUspWarps + warp;
+  uint32_t n = 0, np_row = 0;
+  if (row < A.rows) {
+    const uint32_t np = gather_products<kUspCap>(A, B, (uint32_t)row, S.src[warp], S.aidx[warp]);
+    np_row = np;
+    if (np > (uint32_t)kUspCap) {
+      if (lane == 0) raise_status(ctr, DEV_BIN_OVERFLOW, (uint32_t)row);
+    } else if (np > 128) {
+      n = usp_row_smem(A, B, np, S.src[warp], S.aidx[warp], S.okey[warp], S.oval[warp]);
+    } else if (np > 64) {
+      n = usp_row_regs<4>(A, B, np, S.src[warp], S.aidx[warp], S.okey[warp], S.oval[warp]);
+    } else if (np > 32) {
+      n = usp_row_regs<2>(A, B, np, S.src[warp], S.aidx[warp], S.okey[warp], S.oval[warp]);
+    } else if (np > 0) {
+      n = usp_row_regs<1>(A, B, np, S.src[warp], S.aidx[warp], S.okey[warp], S.oval[warp]);
+    }
+  }
+  if (lane == 0) {
+    S.cnt[warp] = n;
+    S.np[warp] = np_row;
+  }
+  __syncthreads();
+  // warp 0: the tile's aggregate, then a look-back over the preceding tiles,
+  // 32 tiles per read: the nearest tile with an inclusive prefix ends it,
+  // the aggregates of the tiles after it are added; a tile that has not
+  // published yet is polled (bounded)
+  if (warp == 0) {
+    unsigned long long agg = 0;
+    for (int w = 0; w < kUspWarps; ++w) agg += S.cnt[w];
+    unsigned long long prefix = 0;
+    if (t > 0) {
+      if (lane == 0) atomicExch(&tiles[t], kTileAgg | agg);
+      int64_t top = (int64_t)t - 1;  // nearest tile not yet summed
+      int spins = 0;
+      while (top >= 0) {
+        const int64_t j = top - lane;
+        const unsigned long long v = j >= 0 ? ld_volatile_u64(&tiles[j]) : kTileIncl;  // before tile 0: prefix 0
+        const unsigned ready = __ballot_sync(kFull, (v & (kTileAgg | kTileIncl)) != 0);
+        const unsigned incl = __ballot_sync(kFull, (v & kTileIncl) != 0);
+        // lanes up to the nearest inclusive one must all have published
+        const unsigned need = incl ? ((incl & (0u - incl)) << 1) - 1u : kFull;
+        if ((ready & need) != need) {
+          if (++spins > kUspSpinLimit) {
+            if (lane == 0) raise_status(ctr, DEV_SCAN_TIMEOUT, t);
+            break;
+          }
+          __nanosleep(32);
+          continue;
+        }
+        const unsigned long long part = (need >> lane) & 1u ? (v & kTileVal) : 0ull;
+        prefix += warp_sum_u64(part);
+        if (incl) break;
+        top -= 32;
+      }
+    }
+    if (lane == 0) {
+      atomicExch(&tiles[t], kTileIncl | (prefix + agg));
+      S.prefix = prefix;
+      const uint64_t last_row = (uint64_t)t * kUspWarps + kUspWarps;
+      if (last_row >= A.rows) {
+        rowptr64[A.rows] = prefix + agg;
+        if (rowptr32) rowptr32[A.rows] = (uint32_t)(prefix + agg);
+        ctr->total_nnz = prefix + agg;
+      }
+      // class accounting of the tile's rows (stats): ESC1/2/4 by products,
+      // rows of 129-256 products under the small-hash class
+      for (int w = 0; w < kUspWarps; ++w) {
+        if (S.cnt[w] == 0) continue;
+        const uint32_t q = S.np[w];
+        const int c = q <= 32 ? NB_ESC1 : (q <= 64 ? NB_ESC2 : (q <= 128 ? NB_ESC4 : NB_HASH_S));
+        atomicAdd(&ctr->num_count[c], 1u);
+        atomicAdd(&ctr->num_nnz[c], (unsigned long long)S.cnt[w]);
+        atomicAdd(&ctr->num_prod[c], (unsigned long long)q);
+      }
+    }
+  }
+  __syncthreads();
+  if (row < A.rows) {
+    uint64_t off = S.prefix;
+    for (int w = 0; w < warp; ++w) off += S.cnt[w];
+    if (lane == 0) {
+      rowptr64[row] = off;
+      if (rowptr32) rowptr32[row] = (uint32_t)off;
+    }
+    for (uint32_t j = lane; j < n; j += 32) {
+      if (off + j < cap) {
+        c_col[off + j] = S.okey[warp][j];
+        c_val[off + j] = S.oval[warp][j];
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- product enumeration
 // Block-wide, load-balanced enumeration of the products of one row of A.
 //
@@ -1878,6 +2158,7 @@ void set_attrs() {
   allow_smem(k_sym_bitmap<RP>, kSymBitmapSmem);
   allow_smem(k_num_bitmap<RP>, kNumBitmapSmem);
   allow_smem(k_num_window<RP>, kWinNumSmem);
+  allow_smem(k_usp_fused<RP>, sizeof(UspSmem));
   allow_smem(k_sym_hash<RP, 128, 11>, sym_hash_smem<128, 11>());
   allow_smem(k_sym_hash<RP, 256, 13>, sym_hash_smem<256, 13>());
   allow_smem(k_sym_hash<RP, 512, 15>, sym_hash_smem<512, 15>());
@@ -2072,6 +2353,19 @@ int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const O
   return launched;
 }
 
+template <typename RP>
+int launch_usp_fused(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, unsigned long long* tiles, uint64_t cap,
+                     bool rowptr32, uint32_t* c_col, double* c_val, cudaStream_t s) {
+  if (A.rows == 0) return 0;
+  const uint64_t ntiles = (A.rows + kUspWarps - 1) / kUspWarps;
+  cudaMemsetAsync(tiles, 0, ntiles * sizeof(unsigned long long), s);
+  k_usp_fused<RP><<<(unsigned)ntiles, kUspWarps * 32, sizeof(UspSmem), s>>>(
+      A, B, tiles, w.ctr, cap, w.rowptr64, rowptr32 ? w.rowptr32 : nullptr, c_col, c_val);
+  return 1;
+}
+
+uint64_t usp_tiles(uint64_t rows) { return (rows + kUspWarps - 1) / kUspWarps; }
+
 int launch_row_bounds(const DevWork& w, uint32_t* out, cudaStream_t s) {
   if (w.rows == 0) return 0;
   const uint64_t blocks = std::min<uint64_t>((w.rows + 255) / 256, 148ull * 16);
@@ -2144,6 +2438,10 @@ template int launch_hll_rows<uint32_t>(const Csr<uint32_t>&, const DevWork&, int
                                        const uint8_t*, uint32_t*, cudaStream_t);
 template int launch_hll_rows<uint64_t>(const Csr<uint64_t>&, const DevWork&, int, double, uint32_t, bool,
                                        const uint8_t*, uint32_t*, cudaStream_t);
+template int launch_usp_fused<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&,
+                                        unsigned long long*, uint64_t, bool, uint32_t*, double*, cudaStream_t);
+template int launch_usp_fused<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&,
+                                        unsigned long long*, uint64_t, bool, uint32_t*, double*, cudaStream_t);
 template int launch_overflow<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, bool, uint32_t*,
                                        double*, int, cudaStream_t);
 template int launch_overflow<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, bool, uint32_t*,

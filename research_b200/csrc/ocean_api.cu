@@ -9,10 +9,12 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <fstream>
+#include <map>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -91,6 +93,7 @@ struct Stats {
   uint64_t cache_words = 0, cache_used = 0;
   bool cache_dropped = false;
   int bm_kernel = 0;  // numeric bitmap class: 0 no rows, 1 k_num_bitmap (rank + FP64 red), 2 k_num_window
+  bool fused = false;  // ultra-sparse workflow in one fused launch
   int launches = 0;  // kernels launched by the last call
   uint64_t total_est = 0, overflow_rows = 0;
   int hll_log2p = 0;
@@ -197,6 +200,9 @@ struct ocean_handle {
   // saved row bitmaps of the symbolic pass (grow-only, kept across calls)
   unsigned long long* cache_buf = nullptr;
   uint64_t cache_cap_words = 0;
+  // fused ultra-sparse multiply: look-back state per tile (grow-only)
+  unsigned long long* usp_tiles_buf = nullptr;
+  uint64_t usp_tiles_cap = 0;
   // k_num_window: resume cursors per A entry and per-block bitmaps (grow-only)
   uint32_t* win_cursor = nullptr;
   uint64_t win_cursor_cap = 0;
@@ -214,6 +220,7 @@ struct ocean_handle {
     if (out_col) cudaFreeHost(out_col);
     if (out_val) cudaFreeHost(out_val);
     if (cache_buf) cudaFree(cache_buf);
+    if (usp_tiles_buf) cudaFree(usp_tiles_buf);
     if (win_cursor) cudaFree(win_cursor);
     if (win_scratch) cudaFree(win_scratch);
     if (mlp_dev) cudaFree(mlp_dev);
@@ -333,6 +340,7 @@ const char* status_text(unsigned st) {
   if (st & DEV_BIN_OVERFLOW) return "a row exceeded the capacity of its accumulator class";
   if (st & DEV_COUNT_MISMATCH) return "numeric output count differs from the symbolic count";
   if (st & DEV_TC_TIMEOUT) return "a tensor-core completion wait timed out";
+  if (st & DEV_SCAN_TIMEOUT) return "a look-back wait for a preceding tile timed out";
   return "device error";
 }
 
@@ -343,7 +351,8 @@ void check_device_status(ocean_handle* h) {
              h->h_ctr->err_row);
     const unsigned st = h->h_ctr->status;
     throw OceanError{(st & DEV_COUNT_MISMATCH) ? (int)OCEAN_ERR_INTERNAL
-                                               : (st & DEV_TC_TIMEOUT) ? (int)OCEAN_ERR_TIMEOUT : (int)OCEAN_ERR_CAPACITY,
+                                               : (st & (DEV_TC_TIMEOUT | DEV_SCAN_TIMEOUT)) ? (int)OCEAN_ERR_TIMEOUT
+                                                                                            : (int)OCEAN_ERR_CAPACITY,
                      buf};
   }
 }
@@ -874,7 +883,31 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
       // numeric class sizes on the host (grids capped by class size); without
       // them every class is launched at full grid
       bool class_counts = true;
-      if (wf == WF_ULTRASPARSE && readback) {
+      // ultra-sparse rows of at most 256 products: one fused launch writes C
+      // in place (capacity: the product count, read back by the analysis).
+      // Small inputs skip the analysis read-back on the precise path; here
+      // the counters are read back once to see whether the fused path applies.
+      const Config& cf = h->cfg;
+      const bool fusable_cfg = cf.fused_ultrasparse && !cf.estimator_metrics && !cf.use_segment_dispatch &&
+                               (cf.force_workflow == WF_ULTRASPARSE ||
+                                (cf.force_workflow < 0 && cf.use_ultrasparse_workflow));
+      bool fresh = readback;  // h_ctr holds this call's analysis counters
+      if (!readback && fusable_cfg && (wf == WF_PRECISE || wf == WF_ULTRASPARSE)) {
+        OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+        OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
+        fresh = true;
+        mark("fused_probe");
+      }
+      const DevCounters& kc = *h->h_ctr;
+      const bool fits = fresh && kc.max_products <= kUspMaxProducts && kc.total_products < (1ull << 32);
+      if (fits && wf == WF_PRECISE && !readback && cf.force_workflow < 0 &&
+          (double)kc.total_products <= cf.usparse_avg_product_threshold * (double)A.rows)
+        wf = WF_ULTRASPARSE;
+      st.fused = fits && fusable_cfg && wf == WF_ULTRASPARSE;
+      if (st.fused) {
+        nnz = h->h_ctr->total_products;  // C's capacity until the kernel has counted
+        st.total_est = nnz;
+      } else if (wf == WF_ULTRASPARSE && readback) {
         // the estimates are the product counts, whose total the analysis read
         // back and choose_workflow checked against free memory: no read-back
         st.launches += launch_scan(h->w, h->w.est, h->w.est_off, nullptr, &h->w.ctr->total_est, true, np, s,
@@ -893,7 +926,8 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
           OCEAN_CUDA(cudaMemsetAsync(h->w.ctr->num_count, 0, sizeof(unsigned) * NB_COUNT * 2, s));
         }
       }
-      if (wf == WF_PRECISE) {
+      if (st.fused) {
+      } else if (wf == WF_PRECISE) {
         run_symbolic(h, A, B, s, readback, true, true);
         mark("symbolic");
         nnz = h->h_ctr->total_nnz;
@@ -932,7 +966,16 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     alloc_c(h, owner, A.rows, nnz, bits, s);
     mark("alloc_c");
     if (A.rows > 0) {
-      if (wf == WF_PRECISE) {
+      if (st.fused) {
+        grow(h->usp_tiles_buf, h->usp_tiles_cap, usp_tiles(A.rows));
+        // stage events: the fused kernel is reported as the numeric ESC1 stage
+        if (track) record(h, EV_NUM0, s);
+        st.launches += launch_usp_fused(A, B, h->w, h->usp_tiles_buf, nnz, bits == 32, owner->col, owner->val, s);
+        if (track) {
+          for (int i = EV_NUM0 + 1; i <= EV_NUM0 + NB_COUNT; ++i) record(h, i, s);
+          h->ev_mask |= ((1ull << (NB_COUNT + 1)) - 1) << EV_NUM0;
+        }
+      } else if (wf == WF_PRECISE) {
         unsigned num_counts[NB_COUNT];
         for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
         prepare_windows(h, A.nnz, num_counts[NB_BITMAP]);
@@ -960,10 +1003,12 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
     h->ev_recorded = true;
     h->tracked = track;
     mark("launched");
-    if (h->cfg.sync_on_return && A.rows > 0) {
+    if ((h->cfg.sync_on_return || st.fused) && A.rows > 0) {
+      // (the fused path needs the count the kernel wrote: it always waits)
       OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
       OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
       check_device_status(h);
+      if (st.fused) nnz = h->h_ctr->total_nnz;
       mark("synced");
     }
   } catch (...) {
@@ -1068,6 +1113,7 @@ std::string stats_json(ocean_handle* h) {
   o << "\"decision\": {\"workflow\": " << st.workflow << ", \"rowptr_bits\": " << st.rowptr_bits
     << ", \"bitmap_cache_bytes\": " << 8 * st.cache_words << ", \"bitmap_cache_used_bytes\": " << 8 * st.cache_used
     << ", \"bitmap_cache_dropped\": " << (st.cache_dropped ? "true" : "false")
+    << ", \"fused_ultrasparse\": " << (st.fused ? "true" : "false")
     << ", \"numeric_bitmap_kernel\": \"" << (st.bm_kernel == 2 ? "window" : st.bm_kernel == 1 ? "rank" : "none")
     << "\", \"kernel_launches\": " << st.launches << "}, ";
   if (st.sampled)
@@ -1249,6 +1295,8 @@ struct ocean_batch {
   int launches = 0;  // kernels per run
   double tuned_ms = 0.0;
   std::string tuning;  // description of the tuned policy
+  std::string tune_key;     // the batch's autotuning cache key
+  bool tune_cached = false; // the knobs came from the autotuning cache
   DevCounters* h_ctr = nullptr;
 
   uint64_t* pref(int i) const { return d_pref + (uint64_t)i * (n + 1); }
@@ -1485,56 +1533,148 @@ void batch_launch(ocean_batch* b, cudaStream_t s, bool check) {
 // Coordinate search over the class policy on the batch itself: each candidate
 // is planned, captured and timed over `reps` graph launches (CUDA events);
 // the fastest is kept.
-void batch_autotune(ocean_batch* b, cudaStream_t s, int reps) {
-  struct Knob {
-    const char* name;
-    std::vector<double> values;
-  };
-  std::vector<Knob> knobs = {{"esc_max_products", {128, 64, 32}},
-                             {"hash_s_max_scale", {1.0, 0.75, 0.5}},
-                             {"bitmap_words_scale", {1.0, 0.5, 2.0, 4.0}}};
-  cudaEvent_t e0, e1;
-  OCEAN_CUDA(cudaEventCreate(&e0));
-  OCEAN_CUDA(cudaEventCreate(&e1));
-  auto set = [&](const char* k, double v) {
-    if (!strcmp(k, "esc_max_products")) b->cfg.esc_max_products = (int)v;
-    else if (!strcmp(k, "hash_s_max_scale")) b->cfg.hash_s_max_scale = v;
-    else b->cfg.bitmap_words_scale = v;
-  };
-  auto get = [&](const char* k) -> double {
-    if (!strcmp(k, "esc_max_products")) return b->cfg.esc_max_products;
-    if (!strcmp(k, "hash_s_max_scale")) return b->cfg.hash_s_max_scale;
-    return b->cfg.bitmap_words_scale;
-  };
-  auto measure = [&]() -> double {
-    batch_plan_and_capture(b, s);
-    batch_launch(b, s, true);  // warm-up and structure check
-    OCEAN_CUDA(cudaEventRecord(e0, s));
-    for (int i = 0; i < reps; ++i) OCEAN_CUDA(cudaGraphLaunch(b->exec, s));
-    OCEAN_CUDA(cudaEventRecord(e1, s));
-    OCEAN_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    OCEAN_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    return ms / reps;
-  };
-  double best = measure();
-  for (const Knob& k : knobs) {
-    double keep = get(k.name);
-    for (double v : k.values) {
-      if (v == keep) continue;
-      set(k.name, v);
-      const double t = measure();
-      if (t < best) best = t, keep = v;
+// Key of a batch in the autotuning cache: the GPU's name and SM count, the
+// batch's size and its rows and entries (log2 buckets of the totals and of the
+// means per problem and per row), and the workflow options that change which
+// kernels run.
+std::string autotune_key(const ocean_batch* b) {
+  cudaDeviceProp prop;
+  std::string gpu = "unknown";
+  if (cudaGetDeviceProperties(&prop, b->h->device) == cudaSuccess) gpu = prop.name;
+  for (char& c : gpu)
+    if (c == '"' || c == '\\' || c == '\t') c = ' ';
+  auto lg = [](double x) { return x > 0 ? (int)std::floor(std::log2(x) * 2.0) : -1; };  // half-octave buckets
+  const double rows = (double)b->rows, nnz = (double)b->nnz, n = (double)b->n;
+  char buf[256];
+  snprintf(buf, sizeof buf, "%s|sm%d|n%d|rows%d|nnz%d|rpp%d|npr%d|learned%d|wf%d", gpu.c_str(), b->h->num_sms, lg(n),
+           lg(rows), lg(nnz), lg(rows / n), lg(rows > 0 ? nnz / rows : 0.0), b->cfg.use_learned_estimator ? 1 : 0,
+           b->cfg.force_workflow);
+  return buf;
+}
+
+// Tuned knobs of a batch as one flat JSON object (a line of the cache file).
+std::string autotune_line(const std::string& key, const Config& c, double ms) {
+  std::ostringstream o;
+  o.precision(17);
+  o << "{\"key\": \"" << key << "\", \"esc_max_products\": " << c.esc_max_products
+    << ", \"hash_s_max_scale\": " << c.hash_s_max_scale << ", \"bitmap_words_scale\": " << c.bitmap_words_scale
+    << ", \"prefer_direct_hash\": " << (c.prefer_direct_hash ? "true" : "false")
+    << ", \"numeric_windows\": " << (c.numeric_windows ? "true" : "false") << ", \"tuned_ms\": " << ms << "}";
+  return o.str();
+}
+
+// Looks the key up in the cache file; on a hit the knobs go into c.
+bool autotune_lookup(const std::string& path, const std::string& key, Config* c, double* ms) {
+  std::ifstream f(path);
+  if (!f) return false;
+  std::string line;
+  bool hit = false;
+  while (std::getline(f, line)) {
+    if (line.empty()) continue;
+    std::map<std::string, JsonScalar> m;
+    try {
+      m = FlatJson::parse(line);
+    } catch (const std::exception&) {
+      continue;  // a damaged line is skipped
     }
-    set(k.name, keep);
+    auto it = m.find("key");
+    if (it == m.end() || it->second.kind != JsonScalar::kString || it->second.str != key) continue;
+    auto num = [&](const char* k, double d) {
+      auto j = m.find(k);
+      return j != m.end() && j->second.kind == JsonScalar::kNumber ? j->second.num : d;
+    };
+    auto flag = [&](const char* k, bool d) {
+      auto j = m.find(k);
+      return j != m.end() && j->second.kind == JsonScalar::kBool ? j->second.b : d;
+    };
+    c->esc_max_products = (int)num("esc_max_products", c->esc_max_products);
+    c->hash_s_max_scale = num("hash_s_max_scale", c->hash_s_max_scale);
+    c->bitmap_words_scale = num("bitmap_words_scale", c->bitmap_words_scale);
+    c->prefer_direct_hash = flag("prefer_direct_hash", c->prefer_direct_hash);
+    c->numeric_windows = flag("numeric_windows", c->numeric_windows);
+    *ms = num("tuned_ms", 0.0);
+    hit = true;  // the last matching line wins
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  batch_plan_and_capture(b, s);
-  b->tuned_ms = best;
-  char buf[160];
-  snprintf(buf, sizeof buf, "esc_max_products=%d hash_s_max_scale=%g bitmap_words_scale=%g", b->cfg.esc_max_products,
-           b->cfg.hash_s_max_scale, b->cfg.bitmap_words_scale);
+  return hit;
+}
+
+// Coordinate search of the class policy on the batch itself: each knob in
+// turn takes every listed value while the others keep their best, each
+// candidate planned, captured and timed over `reps` graph launches; the
+// fastest is kept and captured. With autotune_cache_file, a batch whose key
+// is in the cache takes the cached knobs without searching, and a search
+// appends its result.
+void batch_autotune(ocean_batch* b, cudaStream_t s, int reps) {
+  const std::string cache = b->cfg.autotune_cache_file;
+  const std::string key = autotune_key(b);
+  b->tune_key = key;
+  double cached_ms = 0.0;
+  if (!cache.empty() && autotune_lookup(cache, key, &b->cfg, &cached_ms)) {
+    batch_plan_and_capture(b, s);
+    b->tuned_ms = cached_ms;
+    b->tune_cached = true;
+  } else {
+    struct Knob {
+      const char* name;
+      std::vector<double> values;
+    };
+    std::vector<Knob> knobs = {{"esc_max_products", {128, 64, 32}},
+                               {"hash_s_max_scale", {1.0, 0.75, 0.5}},
+                               {"bitmap_words_scale", {1.0, 0.5, 2.0, 4.0}},
+                               {"prefer_direct_hash", {1, 0}},
+                               {"numeric_windows", {0, 1}}};
+    cudaEvent_t e0, e1;
+    OCEAN_CUDA(cudaEventCreate(&e0));
+    OCEAN_CUDA(cudaEventCreate(&e1));
+    auto set = [&](const char* k, double v) {
+      if (!strcmp(k, "esc_max_products")) b->cfg.esc_max_products = (int)v;
+      else if (!strcmp(k, "hash_s_max_scale")) b->cfg.hash_s_max_scale = v;
+      else if (!strcmp(k, "bitmap_words_scale")) b->cfg.bitmap_words_scale = v;
+      else if (!strcmp(k, "prefer_direct_hash")) b->cfg.prefer_direct_hash = v != 0.0;
+      else b->cfg.numeric_windows = v != 0.0;
+    };
+    auto get = [&](const char* k) -> double {
+      if (!strcmp(k, "esc_max_products")) return b->cfg.esc_max_products;
+      if (!strcmp(k, "hash_s_max_scale")) return b->cfg.hash_s_max_scale;
+      if (!strcmp(k, "bitmap_words_scale")) return b->cfg.bitmap_words_scale;
+      if (!strcmp(k, "prefer_direct_hash")) return b->cfg.prefer_direct_hash ? 1.0 : 0.0;
+      return b->cfg.numeric_windows ? 1.0 : 0.0;
+    };
+    auto measure = [&]() -> double {
+      batch_plan_and_capture(b, s);
+      batch_launch(b, s, true);  // warm-up and structure check
+      OCEAN_CUDA(cudaEventRecord(e0, s));
+      for (int i = 0; i < reps; ++i) OCEAN_CUDA(cudaGraphLaunch(b->exec, s));
+      OCEAN_CUDA(cudaEventRecord(e1, s));
+      OCEAN_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      OCEAN_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      return ms / reps;
+    };
+    double best = measure();
+    for (const Knob& k : knobs) {
+      double keep = get(k.name);
+      for (double v : k.values) {
+        if (v == keep) continue;
+        set(k.name, v);
+        const double t = measure();
+        if (t < best) best = t, keep = v;
+      }
+      set(k.name, keep);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    batch_plan_and_capture(b, s);
+    b->tuned_ms = best;
+    if (!cache.empty()) {
+      std::ofstream f(cache, std::ios::app);
+      if (f) f << autotune_line(key, b->cfg, best) << "\n";
+    }
+  }
+  char buf[200];
+  snprintf(buf, sizeof buf, "esc_max_products=%d hash_s_max_scale=%g bitmap_words_scale=%g prefer_direct_hash=%d "
+           "numeric_windows=%d%s", b->cfg.esc_max_products, b->cfg.hash_s_max_scale, b->cfg.bitmap_words_scale,
+           b->cfg.prefer_direct_hash ? 1 : 0, b->cfg.numeric_windows ? 1 : 0, b->tune_cached ? " (cached)" : "");
   b->tuning = buf;
 }
 
@@ -1640,6 +1780,20 @@ void batch_outputs(const ocean_batch* b, ocean_csr* C) {
   }
 }
 
+}  // namespace
+
+namespace {
+// Queues the copies of a batch's results into host buffers on s.
+void batch_download(ocean_batch* b, void* rowptrs, uint32_t* col, double* val, cudaStream_t s) {
+  OCEAN_CHECK(b != nullptr && rowptrs != nullptr, OCEAN_ERR_INVALID, "batch or rowptrs is NULL");
+  OCEAN_CHECK(b->c_nnz == 0 || (col && val), OCEAN_ERR_INVALID, "col or val is NULL");
+  OCEAN_CUDA(cudaMemcpyAsync(rowptrs, b->c_rp, (b->rows + b->n) * (uint64_t)(b->out_bits / 8),
+                             cudaMemcpyDeviceToHost, s));
+  if (b->c_nnz) {
+    OCEAN_CUDA(cudaMemcpyAsync(col, b->c_col, b->c_nnz * 4, cudaMemcpyDeviceToHost, s));
+    OCEAN_CUDA(cudaMemcpyAsync(val, b->c_val, b->c_nnz * 8, cudaMemcpyDeviceToHost, s));
+  }
+}
 }  // namespace
 
 extern "C" {
@@ -2075,6 +2229,9 @@ int ocean_batch_info_json(ocean_batch* b, char* buf, size_t cap, size_t* needed)
       << ", \"estimator\": \"" << (b->estimator == 2 ? "learned" : b->estimator == 1 ? "hll" : "none")
       << "\", \"total_est\": " << b->total_est << ", \"kernel_launches\": " << b->launches
       << ", \"graph\": " << (b->exec ? "true" : "false") << ", \"tuned_ms\": " << b->tuned_ms
+      << ", \"tune_cached\": " << (b->tune_cached ? "true" : "false") << ", \"tune_key\": \"" << b->tune_key << "\""
+      << ", \"prefer_direct_hash\": " << (b->cfg.prefer_direct_hash ? "true" : "false")
+      << ", \"numeric_windows\": " << (b->cfg.numeric_windows ? "true" : "false")
       << ", \"esc_max_products\": " << b->cfg.esc_max_products << ", \"hash_s_max_scale\": "
       << b->cfg.hash_s_max_scale << ", \"bitmap_words_scale\": " << b->cfg.bitmap_words_scale
       << ", \"tuning\": \"" << b->tuning << "\"}";
@@ -2085,19 +2242,16 @@ int ocean_batch_info_json(ocean_batch* b, char* buf, size_t cap, size_t* needed)
   });
 }
 
+
 int ocean_batch_download(ocean_batch* b, void* rowptrs, uint32_t* col, double* val, void* stream) {
   return guarded([&] {
-    OCEAN_CHECK(b != nullptr && rowptrs != nullptr, OCEAN_ERR_INVALID, "batch or rowptrs is NULL");
-    OCEAN_CHECK(b->c_nnz == 0 || (col && val), OCEAN_ERR_INVALID, "col or val is NULL");
-    cudaStream_t s = (cudaStream_t)stream;
-    OCEAN_CUDA(cudaMemcpyAsync(rowptrs, b->c_rp, (b->rows + b->n) * (uint64_t)(b->out_bits / 8),
-                               cudaMemcpyDeviceToHost, s));
-    if (b->c_nnz) {
-      OCEAN_CUDA(cudaMemcpyAsync(col, b->c_col, b->c_nnz * 4, cudaMemcpyDeviceToHost, s));
-      OCEAN_CUDA(cudaMemcpyAsync(val, b->c_val, b->c_nnz * 8, cudaMemcpyDeviceToHost, s));
-    }
-    OCEAN_CUDA(cudaStreamSynchronize(s));
+    batch_download(b, rowptrs, col, val, (cudaStream_t)stream);
+    OCEAN_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
   });
+}
+
+int ocean_batch_download_async(ocean_batch* b, void* rowptrs, uint32_t* col, double* val, void* stream) {
+  return guarded([&] { batch_download(b, rowptrs, col, val, (cudaStream_t)stream); });
 }
 
 int ocean_batch_destroy(ocean_batch* b) {

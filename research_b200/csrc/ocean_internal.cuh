@@ -69,7 +69,8 @@ struct DevCounters {
   unsigned int err_row;
   unsigned int num_wide;     // numeric bitmap-class rows whose column span exceeds one 2^20-bit bitmap
   unsigned int wide_cursor;  // queue cursor of those rows' kernel (k_num_bitmap beside k_num_window)
-  unsigned int pad[2];
+  unsigned int usp_tile;     // fused ultra-sparse multiply: tiles handed out
+  unsigned int pad[1];
 };
 
 enum DevError : unsigned int {
@@ -77,7 +78,8 @@ enum DevError : unsigned int {
   DEV_BIN_OVERFLOW = 2u,   // a row did not fit the class it was placed in
   DEV_COUNT_MISMATCH = 4u,  // numeric output count differs from the symbolic count
   DEV_TC_TIMEOUT = 8u,      // a tensor-core completion wait gave up (bounded spin)
-  DEV_BATCH_MISMATCH = 16u  // a batch run needed more room than its plan holds; writes were skipped
+  DEV_BATCH_MISMATCH = 16u, // a batch run needed more room than its plan holds; writes were skipped
+  DEV_SCAN_TIMEOUT = 32u    // a look-back wait for a preceding tile gave up (bounded spin)
 };
 
 constexpr uint32_t kUnknownCount = 0xFFFFFFFFu;

@@ -36,7 +36,7 @@ EXPORTS = (
     "ocean_mlp_features", "ocean_mlp_forward", "ocean_mlp_grad", "ocean_mlp_adam", "ocean_mlp_builtin",
     "ocean_estimate", "ocean_estimate_metrics",
     "ocean_batch_create", "ocean_batch_run", "ocean_batch_launch", "ocean_batch_results", "ocean_batch_info_json",
-    "ocean_batch_destroy", "ocean_spgemm_batched", "ocean_batch_download",
+    "ocean_batch_destroy", "ocean_spgemm_batched", "ocean_batch_download", "ocean_batch_download_async",
 )
 
 MLP_FEATURES = 16
@@ -116,6 +116,7 @@ def lib() -> ctypes.CDLL:
     L.ocean_batch_info_json.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, P(ctypes.c_size_t)]
     L.ocean_batch_destroy.argtypes = [vp]
     L.ocean_batch_download.argtypes = [vp, vp, vp, vp, vp]
+    L.ocean_batch_download_async.argtypes = [vp, vp, vp, vp, vp]
     L.ocean_spgemm_batched.argtypes = [vp, u64, P(CsrView), P(CsrView), P(CsrOut), vp]
     L.ocean_last_error.restype = ctypes.c_char_p
     L.ocean_version.restype = ctypes.c_char_p
@@ -375,9 +376,12 @@ class Batch:
             views.append(d)
         return views
 
-    def download_into(self, rowptrs: np.ndarray, col: np.ndarray, val: np.ndarray, stream: int = 0) -> None:
-        """All results of the last run into (pinned) host arrays, concatenated."""
-        _check(lib().ocean_batch_download(self._h, _ptr(rowptrs), _ptr(col), _ptr(val), stream or None))
+    def download_into(self, rowptrs: np.ndarray, col: np.ndarray, val: np.ndarray, stream: int = 0,
+                      wait: bool = True) -> None:
+        """All results of the last run into (pinned) host arrays, concatenated;
+        wait=False only queues the copies on `stream`."""
+        fn = lib().ocean_batch_download if wait else lib().ocean_batch_download_async
+        _check(fn(self._h, _ptr(rowptrs), _ptr(col), _ptr(val), stream or None))
 
     def info(self) -> dict:
         need = ctypes.c_size_t(0)

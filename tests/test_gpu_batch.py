@@ -142,3 +142,35 @@ def test_one_shot_results_are_owned():
     check(res, As)
     for r in res:
         r.free()
+
+
+def test_autotune_cache_round_trip(tmp_path):
+    # the first plan searches and appends its knobs to the cache file; a
+    # second plan of the same batch takes them from the cache without searching
+    cache = tmp_path / "tune.jsonl"
+    As = mixed_problems(12, seed=300)
+    dA = [DeviceCSR.from_host(a) for a in As]
+    cfg = {"batch_autotune": True, "autotune_cache_file": str(cache)}
+    g1 = SpGEMM(cfg)
+    p1 = Batch(g1, dA)
+    i1 = p1.info()
+    assert i1["tune_cached"] is False and cache.exists()
+    lines = cache.read_text().splitlines()
+    assert len(lines) == 1 and i1["tune_key"] in lines[0]
+    g2 = SpGEMM(cfg)
+    p2 = Batch(g2, dA)
+    i2 = p2.info()
+    assert i2["tune_cached"] is True and i2["tune_key"] == i1["tune_key"]
+    for k in ("esc_max_products", "hash_s_max_scale", "bitmap_words_scale", "prefer_direct_hash", "numeric_windows"):
+        assert i2[k] == i1[k]
+    assert len(cache.read_text().splitlines()) == 1
+    check(p2.run(), As)
+    # a damaged line is skipped, and another batch gets its own key
+    with open(cache, "a") as f:
+        f.write("{not json\n")
+    Bs = mixed_problems(5, seed=301)
+    p3 = Batch(SpGEMM(cfg), [DeviceCSR.from_host(a) for a in Bs])
+    assert p3.info()["tune_cached"] is False
+    check(p3.run(), Bs)
+    for p in (p1, p2, p3):
+        p.close()
