@@ -382,7 +382,54 @@ def run_reference(args, world, rank):
         "note": "the reference has no CPU SpGEMM; this arm times the project's CPU restatement of its "
                 "algorithm on the host cores",
     }
+    if not args.no_extra:
+        line["reference_gpu_build"] = reference_gpu_build()
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_build(names=("laplacian256", "rect")) -> dict:
+    """The reference's own CUDA build (oracle/_ref/spgemm_ref, compiled from
+    its sources with NUM_SM = 148 by `make -C oracle refbin`) on configs 1 and
+    3, through its own driver with 10 warm-up and 10 timed iterations; its
+    stats JSON gives its mean time per multiply. Skipped where the build or a
+    GPU is missing. (Config 2 is not run: nnz(C) exceeds the reference's
+    32-bit row offsets, and a wrapped offset would write out of bounds.)"""
+    import shutil
+    import tempfile
+    ref = ROOT / "oracle" / "_ref" / "spgemm_ref"
+    if not ref.exists() or shutil.which("nvidia-smi") is None:
+        return {"skipped": "reference build or GPU not present"}
+    from research_b200 import matrices as M
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        for name in names:
+            A, B, desc = make_workload(name)
+            pa = Path(td) / "a.mtxd_.hicsr"
+            M.write_hicsr(A, pa)
+            cmd = [str(ref), str(pa)]
+            if B is not A:
+                pb = Path(td) / "b.mtxd_.hicsr"
+                M.write_hicsr(B, pb)
+                cmd.append(str(pb))
+            stats = Path(td) / "stats.json"
+            cfg = Path(td) / "cfg.json"
+            cfg.write_text(json.dumps({"warmup_iters": 10, "bench_iters": 10, "check_correctness": False,
+                                       "output_stats": True, "stats_output_file": str(stats),
+                                       "print_info": False, "track_stage_time": False}))
+            cmd.append(str(cfg))
+            try:
+                r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+                if r.returncode != 0:
+                    out[name] = {"error": f"rc={r.returncode}: {r.stderr[-300:]}"}
+                    continue
+                st = json.loads(stats.read_text())
+                out[name] = {"workload": desc, "reference_ms": round(float(st["total_time"]), 4),
+                             "reference_gflops": round(float(st["gflops"]), 3),
+                             "reference_workflow": st["decision"]["workflow"], "num_sm": 148,
+                             "iterations": "10 warm-up, 10 timed (config/bench.json's counts)"}
+            except Exception as e:  # report, keep the line
+                out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -401,7 +448,7 @@ def run_ours(args, world, rank, local):
         cpu = cpu_sample(A, B, os.cpu_count() or 1, repeats=args.cpu_repeats)
 
     # ---- device-resident throughput (a handle without stage events)
-    g0 = SpGEMM({})
+    g0 = SpGEMM(dict(args.config))
     dA = DeviceCSR.from_host(A)
     dB = dA if same else DeviceCSR.from_host(B)
     for _ in range(args.warmup):
@@ -430,7 +477,7 @@ def run_ours(args, world, rank, local):
     value = world * 2.0 * products * args.steps / (elapsed / 1e3) / 1e9
 
     # ---- per-stage device times (CUDA events per class; a second handle, not in the timed region)
-    g = SpGEMM({"track_stage_time": True})
+    g = SpGEMM({**args.config, "track_stage_time": True})
     classes = ("esc1", "esc2", "esc4", "hash_s", "hash_m", "hash_l", "bitmap")
     stage_names = ["analysis", "scan"] + [f"symbolic_{c}" for c in classes] + [f"numeric_{c}" for c in classes]
     stage_ms = {k: 0.0 for k in stage_names}
@@ -991,6 +1038,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="headline workload only (no configs 1, 3, 4, 5)")
+    ap.add_argument("--config", type=json.loads, default={},
+                    help="library configuration (JSON object) for the headline workload's handles, e.g. "
+                         "'{\"numeric_windows\": true}' when profiling a kernel variant")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("note: fewer than 3 warm-up steps", file=sys.stderr)

@@ -1286,7 +1286,8 @@ __global__ void __launch_bounds__(NT) k_num_hash(Csr<RP> A, Csr<RP> B, RowQueue 
 // select. Warp-collective; emit runs on the lanes that own an entry.
 constexpr uint32_t kSparseBits = 8;
 template <typename Emit>
-__device__ __forceinline__ void warp_emit_group(unsigned long long word, int lane, Emit&& emit) {
+__device__ __forceinline__ void warp_emit_group(unsigned long long word, int lane, Emit&& emit,
+                                                uint32_t jlo = 0u, uint32_t jhi = 0xFFFFFFFFu) {
   const uint32_t cnt = (uint32_t)__popcll(word);
   uint32_t incl = cnt;
 #pragma unroll
@@ -1296,20 +1297,22 @@ __device__ __forceinline__ void warp_emit_group(unsigned long long word, int lan
   }
   const uint32_t excl = incl - cnt;
   const uint32_t total = __shfl_sync(kFull, incl, 31);
-  if (total == 0) return;
+  jhi = min(jhi, total);
+  if (jlo >= jhi) return;
   if (__reduce_max_sync(kFull, cnt) <= kSparseBits) {
     uint32_t j = excl;
     unsigned long long x = word;
     while (x) {
       const uint32_t b = (uint32_t)(__ffsll((long long)x) - 1);
       x &= x - 1ull;
-      emit(j++, (uint32_t)lane * 64u + b);
+      if (j >= jlo && j < jhi) emit(j, (uint32_t)lane * 64u + b);
+      ++j;
     }
     return;
   }
-  const uint32_t rounds = (total + 31) >> 5;
+  const uint32_t rounds = (jhi - jlo + 31) >> 5;
   for (uint32_t rd = 0; rd < rounds; ++rd) {
-    const uint32_t j = rd * 32 + lane;
+    const uint32_t j = jlo + rd * 32 + lane;
     uint32_t k = 0;
 #pragma unroll
     for (int step = 16; step > 0; step >>= 1) {
@@ -1318,7 +1321,7 @@ __device__ __forceinline__ void warp_emit_group(unsigned long long word, int lan
     }
     unsigned long long x = __shfl_sync(kFull, word, k);
     uint32_t r = j - __shfl_sync(kFull, excl, k);
-    if (j < total) {
+    if (j < jhi) {
       uint32_t pos = 0;
 #pragma unroll
       for (int sb = 32; sb > 0; sb >>= 1) {
@@ -1519,19 +1522,36 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
         run += __shfl_sync(kFull, x, 31);
       }
       __syncthreads();
-      // ordered output of the column ids (and zeroed values), a warp per
-      // group of 32 words
-      for (uint32_t wb = (uint32_t)warp * 32u; wb < nwords; wb += 32u * (kBitmapThreads / 32)) {
-        const uint32_t w = wb + lane;
-        const uint64_t gout = off + S.spre[wb >> 10] + S.wpre[wb];
-        const uint64_t gcol = w0 + (uint64_t)wb * 64;
-        warp_emit_group(w < nwords ? S.bits[w] : 0ull, lane, [&](uint32_t j, uint32_t b) {
-          const uint64_t o = gout + j;
-          if (o < row_lim) {
-            c_col[o] = (uint32_t)(gcol + b);
-            c_val[o] = 0.0;
+      // ordered output of the column ids (and zeroed values): warp w writes
+      // the window's entries [w n / 32, (w + 1) n / 32), starting at the word
+      // that holds its first entry, 32 words at a time. Split by entries, not
+      // by words: the dense words of a power-law row's hub columns would
+      // otherwise all fall to the first few warps.
+      {
+        const uint32_t e0 = (uint32_t)(((uint64_t)warp * nw_total) >> 5);
+        const uint32_t e1 = (uint32_t)(((uint64_t)(warp + 1) * nw_total) >> 5);
+        if (e0 < e1) {
+          // last word whose prefix is <= e0
+          uint32_t lo_w = 0, hi_w = nwords;  // prefix(lo_w) <= e0 < prefix(hi_w) (prefix(nwords) = total)
+          while (hi_w - lo_w > 1) {
+            const uint32_t mid = (lo_w + hi_w) >> 1;
+            if (S.spre[mid >> 10] + (uint32_t)S.wpre[mid] <= e0) lo_w = mid; else hi_w = mid;
           }
-        });
+          for (uint32_t wb = lo_w; wb < nwords; wb += 32u) {
+            const uint32_t gpre = S.spre[wb >> 10] + S.wpre[wb];
+            if (gpre >= e1) break;
+            const uint32_t w = wb + lane;
+            const uint64_t gout = off + gpre;
+            const uint64_t gcol = w0 + (uint64_t)wb * 64;
+            warp_emit_group(w < nwords ? S.bits[w] : 0ull, lane, [&](uint32_t j, uint32_t b) {
+              const uint64_t o = gout + j;
+              if (o < row_lim) {
+                c_col[o] = (uint32_t)(gcol + b);
+                c_val[o] = 0.0;
+              }
+            }, e0 > gpre ? e0 - gpre : 0u, e1 - gpre);
+          }
+        }
       }
       __syncthreads();
       // pass 2: accumulate values at their ranks
@@ -1783,20 +1803,33 @@ __global__ void __launch_bounds__(kBitmapThreads, 1)
       // from the slots (which are cleared for the next window)
       const uint64_t wout = row_off + r0;
       const uint64_t row_lim = row_off + expect;
-      for (uint32_t wb = (uint32_t)warp * 32u; wb < we; wb += 32u * (NT / 32)) {
-        const uint32_t w = wb + lane;
-        const uint32_t gpre = S.wpre[wb];
-        const uint64_t gcol = ca + (uint64_t)wb * 64;
-        warp_emit_group(w < we ? wbits[w] : 0ull, lane, [&](uint32_t j, uint32_t b) {
-          const uint32_t lr = gpre + j;
-          const uint64_t at = wout + lr;
-          const double v = vals[lr];
-          vals[lr] = 0.0;
-          if (at < row_lim) {
-            c_col[at] = (uint32_t)(gcol + b);
-            c_val[at] = v;
-          }
-        });
+      // split by entries across the warps (dense hub words would otherwise
+      // all fall to the first warps), 32 words at a time from the word that
+      // holds each warp's first entry
+      const uint32_t e0 = (uint32_t)(((uint64_t)warp * nwin) / (NT / 32));
+      const uint32_t e1 = (uint32_t)(((uint64_t)(warp + 1) * nwin) / (NT / 32));
+      if (e0 < e1) {
+        uint32_t lo_w = 0, hi_w = we;  // prefix(lo_w) <= e0 < prefix(hi_w) (prefix(we) = nwin)
+        while (hi_w - lo_w > 1) {
+          const uint32_t mid = (lo_w + hi_w) >> 1;
+          if ((uint32_t)S.wpre[mid] <= e0) lo_w = mid; else hi_w = mid;
+        }
+        for (uint32_t wb = lo_w; wb < we; wb += 32u) {
+          const uint32_t gpre = S.wpre[wb];
+          if (gpre >= e1) break;
+          const uint32_t w = wb + lane;
+          const uint64_t gcol = ca + (uint64_t)wb * 64;
+          warp_emit_group(w < we ? wbits[w] : 0ull, lane, [&](uint32_t j, uint32_t b) {
+            const uint32_t lr = gpre + j;
+            const uint64_t at = wout + lr;
+            const double v = vals[lr];
+            vals[lr] = 0.0;
+            if (at < row_lim) {
+              c_col[at] = (uint32_t)(gcol + b);
+              c_val[at] = v;
+            }
+          }, e0 > gpre ? e0 - gpre : 0u, e1 - gpre);
+        }
       }
       __syncthreads();
       r0 += nwin;
