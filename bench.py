@@ -65,6 +65,13 @@ def make_workload(name: str):
         p, _, _ = O.row_stats(A, A)
         rows = np.nonzero((p > 16384) & (p < 1_000_000))[0][::32]
         return take_rows(A, rows), A, f"{rows.size} typical heavy rows of R-MAT n=2^20 (every 32nd with 16384 < products < 1e6) times A"
+    if name == "rmat20s":
+        # reduced case with the full workload's row mix (every class): every
+        # 64th row of the R-MAT 2^20 matrix times the whole matrix; per-launch
+        # counters of the full workload are these times ~64
+        A = M.rmat(20, 16, (0.57, 0.19, 0.19, 0.05), seed=0)
+        rows = np.arange(0, A.rows, 64)
+        return take_rows(A, rows), A, f"{rows.size} rows of R-MAT n=2^20 (every 64th) times A"
     if name.startswith("rmat"):
         sc = int(name[4:])
         A = M.rmat(sc, 16, (0.57, 0.19, 0.19, 0.05), seed=0)
@@ -579,7 +586,7 @@ def run_ours(args, world, rank, local):
     configs = None
     if world == 1 and not args.no_extra:
         del dA, dB
-        torch.cuda.empty_cache()
+        release_memory()
         configs = extra_legs(args, stream)
 
     if rank != 0:
@@ -760,6 +767,13 @@ def leg_small(name: str, stream, steps: int = 20, warmup: int = 5, check: bool =
     out["e2e_ms"] = round(e2e_ms, 4)
     out["e2e_gflops"] = round(2.0 * products / e2e_ms / 1e6, 3)
     g.close()
+    # CPU baseline of the whole product (OpenMP Gustavson, all host cores; median of 5)
+    threads = os.cpu_count() or 1
+    cpu_gustavson(A, B, threads)
+    ts = sorted(cpu_gustavson(A, B, threads)[0] for _ in range(5))
+    out["cpu_ms"] = round(1e3 * ts[2], 3)
+    out["cpu_gflops"] = round(2.0 * products / ts[2] / 1e9, 3)
+    out["cpu_cores"] = threads
     return out
 
 
@@ -851,7 +865,14 @@ def leg_batch(stream, steps: int = 3, warmup: int = 2, e2e_steps: int = 2, ablat
                     worst = max(worst, O.compare(h.rowptr, h.col, h.val, rp, cj, cx, ca, 1e-12))
                 rec["parity"] = {"problems_checked": len(range(0, 512, 37)), "max_rel_err": worst}
             if e2e_steps > 0:
-                rec["e2e"] = batch_e2e(plan, info, dA, gp, stream, e2e_steps)
+                hosts = [(pinned_like(a.rowptr), pinned_like(a.col), pinned_like(a.val)) for a in dA]
+                nnz_c = int(info["nnz_c"])
+                wide = info["rowptr_bits"] == 64
+                outs = (torch.empty(int(info["rows"]) + len(dA), dtype=torch.int64 if wide else torch.int32,
+                                    pin_memory=True),
+                        torch.empty(max(nnz_c, 1), dtype=torch.int32, pin_memory=True),
+                        torch.empty(max(nnz_c, 1), dtype=torch.float64, pin_memory=True))
+                rec["e2e"] = batch_e2e(plan, info, dA, gp, stream, e2e_steps, hosts, outs)
                 out["plain"]["e2e_ms"] = rec["e2e"].pop("plain_ms")
                 out["plain"]["e2e_gflops"] = gf(out["plain"]["e2e_ms"])
                 rec["e2e"]["gflops"] = gf(rec["e2e"]["ms"])
@@ -864,7 +885,9 @@ def leg_batch(stream, steps: int = 3, warmup: int = 2, e2e_steps: int = 2, ablat
             # pipelined over three streams: inputs of plan i+1 copied in and
             # plan i computed while plan i-1's results are copied back
             tuned = {k: info[k] for k in ("esc_max_products", "hash_s_max_scale", "bitmap_words_scale") if k in info}
-            pe = batch_e2e_pipelined(dA, {"use_learned_estimator": True, **tuned}, stream, e2e_steps, chunks=8)
+            pe = batch_e2e_pipelined(dA, {"use_learned_estimator": True, **tuned}, stream, e2e_steps, hosts, outs,
+                                     chunks=8)
+            del hosts, outs
             pe["gflops"] = gf(pe["ms"])
             rec["e2e_pipelined"] = pe
             rec["e2e_pipelined_speedup_vs_plain"] = round(out["plain"]["e2e_ms"] / pe["ms"], 3)
@@ -872,21 +895,19 @@ def leg_batch(stream, steps: int = 3, warmup: int = 2, e2e_steps: int = 2, ablat
     return out
 
 
-def batch_e2e(plan, info, dA, gp, stream, steps: int) -> dict:
-    """End-to-end ms of one batched step and of 512 plain host-buffer calls."""
+def pinned_like(t):
+    import torch
+    return torch.empty(t.shape, dtype=t.dtype, pin_memory=True).copy_(t.cpu())
+
+
+def batch_e2e(plan, info, dA, gp, stream, steps: int, hosts, outs) -> dict:
+    """End-to-end ms of one batched step and of 512 plain host-buffer calls
+    (hosts: pinned copies of the inputs; outs: pinned rowptr, col, val arrays)."""
     import torch
     from research_b200.ocean import CsrOut, HostCSR, _check, lib
     sptr = stream.cuda_stream
-
-    def pinned_like(t):
-        return torch.empty(t.shape, dtype=t.dtype, pin_memory=True).copy_(t.cpu())
-    hosts = [(pinned_like(a.rowptr), pinned_like(a.col), pinned_like(a.val)) for a in dA]
     nnz_c = int(info["nnz_c"])
-    rows_tot = int(info["rows"])
-    rp_out = torch.empty(rows_tot + len(dA), dtype=torch.int64 if info["rowptr_bits"] == 64 else torch.int32,
-                         pin_memory=True)
-    col_out = torch.empty(max(nnz_c, 1), dtype=torch.int32, pin_memory=True)
-    val_out = torch.empty(max(nnz_c, 1), dtype=torch.float64, pin_memory=True)
+    rp_out, col_out, val_out = outs
 
     def step():
         for a, (r, c, v) in zip(dA, hosts):
@@ -912,7 +933,7 @@ def batch_e2e(plan, info, dA, gp, stream, steps: int) -> dict:
                    "plain: 512 x ocean_spgemm_host"}
 
 
-def batch_e2e_pipelined(dA, config: dict, stream, steps: int, chunks: int = 8) -> dict:
+def batch_e2e_pipelined(dA, config: dict, stream, steps: int, hosts, outs, chunks: int = 8) -> dict:
     """End-to-end ms of one step of the batch as `chunks` captured plans on
     three streams (copy in, compute, copy out; ocean_batch_launch and
     ocean_batch_download_async), CUDA events on `stream` around the step."""
@@ -927,17 +948,20 @@ def batch_e2e_pipelined(dA, config: dict, stream, steps: int, chunks: int = 8) -
         plans.append(Batch(g, part, stream=stream.cuda_stream))
         parts.append(part)
     infos = [pl.info() for pl in plans]
-
-    def pinned_like(t):
-        return torch.empty(t.shape, dtype=t.dtype, pin_memory=True).copy_(t.cpu())
-    hosts = [[(pinned_like(a.rowptr), pinned_like(a.col), pinned_like(a.val)) for a in part] for part in parts]
-    outs = []
+    # each plan's inputs are slices of the pinned input copies; its results go
+    # to consecutive slices of the shared pinned outputs (row pointers as
+    # 64-bit words, enough for either width)
+    chunk_hosts = [hosts[bounds[i]:bounds[i + 1]] for i in range(chunks)]
+    rp_all, col_all, val_all = outs
+    rp64 = rp_all.view(torch.int64) if rp_all.dtype == torch.int64 else None
+    chunk_outs, e_at, r_at = [], 0, 0
     for inf in infos:
-        wide = inf["rowptr_bits"] == 64
-        outs.append((torch.empty(int(inf["rows"]) + int(inf["problems"]), dtype=torch.int64 if wide else torch.int32,
-                                 pin_memory=True),
-                     torch.empty(max(int(inf["nnz_c"]), 1), dtype=torch.int32, pin_memory=True),
-                     torch.empty(max(int(inf["nnz_c"]), 1), dtype=torch.float64, pin_memory=True)))
+        nnz, nr = int(inf["nnz_c"]), int(inf["rows"]) + int(inf["problems"])
+        rp_view = (torch.empty(nr, dtype=torch.int64 if inf["rowptr_bits"] == 64 else torch.int32, pin_memory=True)
+                   if rp64 is None or inf["rowptr_bits"] != 64 else rp64[r_at:r_at + nr])
+        chunk_outs.append((rp_view, col_all[e_at:e_at + max(nnz, 1)], val_all[e_at:e_at + max(nnz, 1)]))
+        e_at += nnz
+        r_at += nr
     s_in, s_comp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
 
     def step():
@@ -946,7 +970,7 @@ def batch_e2e_pipelined(dA, config: dict, stream, steps: int, chunks: int = 8) -
         for st in (s_in, s_comp, s_out):
             st.wait_event(start)
         done = None
-        for pl, part, hs, (rp, col, val) in zip(plans, parts, hosts, outs):
+        for pl, part, hs, (rp, col, val) in zip(plans, parts, chunk_hosts, chunk_outs):
             with torch.cuda.stream(s_in):
                 for a, (r, c, v) in zip(part, hs):
                     a.rowptr.copy_(r, non_blocking=True)
@@ -965,8 +989,8 @@ def batch_e2e_pipelined(dA, config: dict, stream, steps: int, chunks: int = 8) -
         stream.wait_event(done)
     ms = time_on_device(step, steps, 1, stream)
     res = {"ms": round(ms, 3), "chunks": chunks, "kernel_launches_per_plan": infos[0]["kernel_launches"],
-           "h2d_bytes_per_step": int(sum(x.nbytes for hs in hosts for h in hs for x in h)),
-           "d2h_bytes_per_step": int(sum(o[0].nbytes + 12 * int(inf["nnz_c"]) for o, inf in zip(outs, infos))),
+           "h2d_bytes_per_step": int(sum(x.nbytes for h in hosts for x in h)),
+           "d2h_bytes_per_step": int(sum(o[0].nbytes + 12 * int(inf["nnz_c"]) for o, inf in zip(chunk_outs, infos))),
            "api": "8 x (ocean_batch_create once; per step ocean_batch_launch, ocean_batch_download_async) "
                   "on copy-in/compute/copy-out streams"}
     for pl in plans:
@@ -988,9 +1012,20 @@ def extra_legs(args, stream) -> dict:
         except Exception as e:  # report, keep the headline line
             out[name] = {"error": f"{type(e).__name__}: {e}"}
         out[name]["leg_seconds"] = round(time.time() - t0, 1)
-        import torch
-        torch.cuda.empty_cache()
+        release_memory()
     return out
+
+
+def release_memory():
+    """Returns cached device memory and torch's cached pinned host buffers
+    (a leg pins up to ~120 GB of host memory for its copies)."""
+    import gc
+    import torch
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    if hasattr(torch._C, "_host_emptyCache"):
+        torch._C._host_emptyCache()
 
 
 
