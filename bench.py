@@ -65,13 +65,21 @@ def make_workload(name: str):
         p, _, _ = O.row_stats(A, A)
         rows = np.nonzero((p > 16384) & (p < 1_000_000))[0][::32]
         return take_rows(A, rows), A, f"{rows.size} typical heavy rows of R-MAT n=2^20 (every 32nd with 16384 < products < 1e6) times A"
-    if name == "rmat20s":
-        # reduced case with the full workload's row mix (every class): every
-        # 64th row of the R-MAT 2^20 matrix times the whole matrix; per-launch
-        # counters of the full workload are these times ~64
+    if name == "rmat20h":
+        # profiling case weighted to heavy rows: every 64th row of the R-MAT
+        # 2^20 matrix (ids with six low zero bits, ~9x the mean products) times A
         A = M.rmat(20, 16, (0.57, 0.19, 0.19, 0.05), seed=0)
         rows = np.arange(0, A.rows, 64)
-        return take_rows(A, rows), A, f"{rows.size} rows of R-MAT n=2^20 (every 64th) times A"
+        return take_rows(A, rows), A, f"{rows.size} rows of R-MAT n=2^20 (every 64th, heavy-weighted) times A"
+    if name == "rmat20s":
+        # reduced case with the full workload's row mix (every class): a seeded
+        # uniform sample of 1/64 of the rows of the R-MAT 2^20 matrix times the
+        # whole matrix; its products and output entries are ~1/64 of the full
+        # multiply's (a fixed stride would not do: R-MAT row weights grow with
+        # the zero bits of the row id, so every 64th row is a heavy row)
+        A = M.rmat(20, 16, (0.57, 0.19, 0.19, 0.05), seed=0)
+        rows = np.sort(np.random.default_rng(64).choice(A.rows, A.rows // 64, replace=False))
+        return take_rows(A, rows), A, f"{rows.size} rows of R-MAT n=2^20 (seeded uniform 1/64 sample) times A"
     if name.startswith("rmat"):
         sc = int(name[4:])
         A = M.rmat(sc, 16, (0.57, 0.19, 0.19, 0.05), seed=0)

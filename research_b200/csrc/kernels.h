@@ -38,6 +38,14 @@ struct DevWork {
   uint32_t* win_cursor = nullptr;
   unsigned long long* win_scratch = nullptr;
   uint32_t wide_rows = 0xFFFFFFFFu;
+  // rows of A with more than kLongRowEntries entries: listed by the analysis
+  // and summarised (and HLL-merged) by all warps together; null: each row is
+  // handled by its own lane group
+  uint32_t* long_rows = nullptr;
+  LongRowAcc* long_acc = nullptr;
+  uint32_t long_cap = 0;
+  uint32_t* long_chunk_row = nullptr;  // chunk id -> index in long_rows
+  uint32_t long_chunk_cap = 0;
   // segment-driven dispatch: per-row policy slot (0: the call's policy,
   // 1 + SegClass: that segment class's policy); null: slot 0 for every row
   const uint8_t* row_pol = nullptr;

@@ -127,9 +127,64 @@ __device__ __forceinline__ uint32_t spread_index(uint32_t idx, uint32_t count, u
 }
 
 // ---------------------------------------------------------------- analysis
+// Products, smallest first column, largest last column and longest B row
+// over A entries k0, k0 + G, k0 + 2G, ... below k1, accumulated into p, mn,
+// mx, lb. Four entries per pass have their dependent loads in flight together.
+template <int G, typename RP>
+__device__ __forceinline__ void span_part(const Csr<RP>& A, const Csr<RP>& B, uint64_t k0, uint64_t k1,
+                                          unsigned long long& p, uint32_t& mn, uint32_t& mx, uint32_t& lb) {
+  for (; k0 < k1; k0 += 4 * G) {
+    uint32_t j[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) j[u] = k0 + (uint64_t)u * G < k1 ? A.col[k0 + (uint64_t)u * G] : kEmpty;
+    uint64_t b0[4], b1[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      b0[u] = b1[u] = 0;
+      if (j[u] != kEmpty) {
+        b0[u] = B.row_begin(j[u]);
+        b1[u] = B.row_end(j[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (b1[u] > b0[u]) {
+        p += b1[u] - b0[u];
+        mn = min(mn, B.col[b0[u]]);
+        mx = max(mx, B.col[b1[u] - 1]);
+        lb = max(lb, (uint32_t)min(b1[u] - b0[u], (uint64_t)0xFFFFFFFFu));
+      }
+    }
+  }
+}
+
+// The analysis results of one row: per-row arrays, and whether and where it
+// joins a symbolic class (-1: no product, no class).
+__device__ __forceinline__ int analysis_write(uint64_t row, uint64_t a_len, unsigned long long p, uint32_t mn,
+                                              uint32_t mx, uint32_t lb, uint32_t* __restrict__ prod,
+                                              uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
+                                              uint32_t* __restrict__ anz, uint32_t* __restrict__ maxb,
+                                              uint32_t* __restrict__ row_nnz, uint64_t* __restrict__ bm_off,
+                                              const SymPolicySet& pols, const uint8_t* __restrict__ row_pol) {
+  prod[row] = p > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)p;
+  lo[row] = mn;
+  hi[row] = mx;
+  anz[row] = (uint32_t)a_len;
+  maxb[row] = lb;
+  bm_off[row] = ~0ull;
+  if (p == 0) {
+    row_nnz[row] = 0;
+    return -1;
+  }
+  return sym_bin_for(p, (uint64_t)mx - mn + 1, pols.p[row_pol ? row_pol[row] : 0]);
+}
+
 // One group of G lanes per row of A: products, output column span; then the
 // row is appended to its symbolic class list (rows with no product get
-// row_nnz = 0 here and no class).
+// row_nnz = 0 here and no class). A block covers 256 / G consecutive rows; its
+// class-list append and totals cost one global atomic per class and block.
+// Rows longer than kLongRowEntries are only listed here (when the list
+// exists) and summarised by k_analysis_long.
 template <typename RP, int G>
 __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
                                                   uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
@@ -137,13 +192,23 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
                                                   uint32_t* __restrict__ row_nnz, uint64_t* __restrict__ bm_off,
                                                   uint32_t* __restrict__ sym_bins,
                                                   DevCounters* __restrict__ ctr, SymPolicySet pols,
-                                                  const uint8_t* __restrict__ row_pol) {
-  __shared__ unsigned long long s_anz[SB_COUNT], s_prod[SB_COUNT], s_words;
+                                                  const uint8_t* __restrict__ row_pol,
+                                                  uint32_t* __restrict__ long_rows,
+                                                  LongRowAcc* __restrict__ long_acc, uint32_t long_cap,
+                                                  uint32_t* __restrict__ long_chunk_row, uint32_t chunk_cap) {
+  __shared__ unsigned long long s_anz[SB_COUNT], s_prod[SB_COUNT], s_words, s_tot;
+  __shared__ unsigned s_maxp, s_maxa, s_cnt[SB_COUNT];
   if (threadIdx.x < SB_COUNT) {
     s_anz[threadIdx.x] = 0ull;
     s_prod[threadIdx.x] = 0ull;
+    s_cnt[threadIdx.x] = 0u;
   }
-  if (threadIdx.x == 0) s_words = 0ull;
+  if (threadIdx.x == 0) {
+    s_words = 0ull;
+    s_tot = 0ull;
+    s_maxp = 0u;
+    s_maxa = 0u;
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int sl = lane & (G - 1);
@@ -154,18 +219,10 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
     a0 = A.row_begin(row);
     a1 = A.row_end(row);
   }
+  const bool is_long = long_acc != nullptr && a1 - a0 > kLongRowEntries;  // uniform in the group
   unsigned long long p = 0;
   uint32_t mn = kEmpty, mx = 0, lb = 0;
-  for (uint64_t k = a0 + sl; k < a1; k += G) {
-    const uint32_t j = A.col[k];
-    const uint64_t b0 = B.row_begin(j), b1 = B.row_end(j);
-    if (b1 > b0) {
-      p += b1 - b0;
-      mn = min(mn, B.col[b0]);
-      mx = max(mx, B.col[b1 - 1]);
-      lb = max(lb, (uint32_t)min(b1 - b0, (uint64_t)0xFFFFFFFFu));
-    }
-  }
+  if (!is_long) span_part<G>(A, B, a0 + sl, a1, p, mn, mx, lb);
 #pragma unroll
   for (int o = G / 2; o > 0; o >>= 1) {
     p += __shfl_xor_sync(kFull, p, o);
@@ -176,66 +233,158 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
   int b = -1;
   const bool leader = valid && sl == 0;
   if (leader) {
-    prod[row] = p > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)p;
-    lo[row] = mn;
-    hi[row] = mx;
-    anz[row] = (uint32_t)(a1 - a0);
-    maxb[row] = lb;
-    bm_off[row] = ~0ull;
-    if (p == 0) {
-      row_nnz[row] = 0;
+    if (a1 > a0) atomicMax(&s_maxa, (unsigned)(a1 - a0));
+    if (is_long) {
+      // list the row and give it its chunk ids (the list holds nnz(A) / 512 + 1
+      // rows and the map nnz(A) / 256 + that many chunks, so both always fit)
+      const uint32_t nch = (uint32_t)((a1 - a0 + kLongChunk - 1) / kLongChunk);
+      const unsigned i = atomicAdd(&ctr->num_long, 1u);
+      const unsigned base = i < long_cap ? atomicAdd(&ctr->long_chunks, nch) : 0u;
+      if (i < long_cap && (uint64_t)base + nch <= chunk_cap) {
+        long_rows[i] = (uint32_t)row;
+        LongRowAcc& L = long_acc[i];
+        L.prod = 0ull;
+        L.lo = kEmpty;
+        L.hi = 0u;
+        L.maxb = 0u;
+        L.done = 0u;
+        L.hdone = 0u;
+        L.base = base;
+        for (int r = 0; r < 64; ++r) L.reg[r] = 0u;
+        for (uint32_t c = 0; c < nch; ++c) long_chunk_row[base + c] = i;
+      } else {
+        raise_status(ctr, DEV_BIN_OVERFLOW, (uint32_t)row);
+      }
     } else {
-      const uint64_t span = (uint64_t)mx - mn + 1;
-      b = sym_bin_for(p, span, pols.p[row_pol ? row_pol[row] : 0]);
+      b = analysis_write(row, a1 - a0, p, mn, mx, lb, prod, lo, hi, anz, maxb, row_nnz, bm_off, pols, row_pol);
+      // totals for stats and the workflow decision
+      if (p) {
+        atomicAdd(&s_tot, p);
+        atomicMax(&s_maxp, p > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned)p);
+      }
     }
   }
   {
-    // per-class sums: warp reductions first, one shared atomic per warp and class
+    // per-class sums: shared atomics of the leaders (G = 32: one row per
+    // warp), or one per warp and class present in the warp
     const unsigned long long my_anz = (b >= 0) ? (unsigned long long)(a1 - a0) : 0ull;
     const unsigned long long my_p = (b >= 0) ? p : 0ull;
     const uint64_t span = (uint64_t)mx - mn + 1;
     const unsigned long long my_w = (b == SB_BITMAP && span <= kBitmapBits) ? ((span + 63) >> 6) : 0ull;
-#pragma unroll
-    for (int c = 0; c < SB_COUNT; ++c) {
-      const unsigned long long sa = warp_sum_u64(b == c ? my_anz : 0ull);
-      const unsigned long long sp = warp_sum_u64(b == c ? my_p : 0ull);
-      if (lane == 0 && sp) {
-        atomicAdd(&s_anz[c], sa);
-        atomicAdd(&s_prod[c], sp);
+    if (G == 32) {
+      if (b >= 0) {
+        atomicAdd(&s_anz[b], my_anz);
+        atomicAdd(&s_prod[b], my_p);
+        if (my_w) atomicAdd(&s_words, my_w);
+      }
+    } else {
+      unsigned present = __reduce_or_sync(kFull, b >= 0 ? 1u << b : 0u);
+      while (present) {
+        const int c = __ffs(present) - 1;
+        present &= present - 1;
+        const unsigned long long sa = warp_sum_u64(b == c ? my_anz : 0ull);
+        const unsigned long long sp = warp_sum_u64(b == c ? my_p : 0ull);
+        if (lane == 0 && sp) {
+          atomicAdd(&s_anz[c], sa);
+          atomicAdd(&s_prod[c], sp);
+        }
+      }
+      if (__any_sync(kFull, my_w != 0)) {
+        const unsigned long long sw = warp_sum_u64(my_w);
+        if (lane == 0 && sw) atomicAdd(&s_words, sw);
       }
     }
-    const unsigned long long sw = warp_sum_u64(my_w);
-    if (lane == 0 && sw) atomicAdd(&s_words, sw);
   }
-  bin_append(b, (uint32_t)row, ctr->sym_count, sym_bins, A.rows);
-  // totals for stats and the workflow decision
-  unsigned long long tp = leader ? p : 0ull;
-  tp = warp_sum_u64(tp);
-  unsigned mp = leader ? (p > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned)p) : 0u;
-  unsigned ma = leader ? (unsigned)(a1 - a0) : 0u;
-  mp = __reduce_max_sync(kFull, mp);
-  ma = __reduce_max_sync(kFull, ma);
-  if (lane == 0) {
-    if (tp) atomicAdd(&ctr->total_products, tp);
-    if (mp) atomicMax(&ctr->max_products, mp);
-    if (ma) atomicMax(&ctr->max_a_nnz, ma);
+  {
+    const int bq[1] = {b};
+    const uint32_t rq[1] = {(uint32_t)row};
+    block_bin_append<1>(bq, rq, s_cnt, SB_COUNT, ctr->sym_count, sym_bins, A.rows);
   }
-  __syncthreads();
   if (threadIdx.x < SB_COUNT) {
     if (s_anz[threadIdx.x]) atomicAdd(&ctr->sym_anz[threadIdx.x], s_anz[threadIdx.x]);
     if (s_prod[threadIdx.x]) atomicAdd(&ctr->sym_prod[threadIdx.x], s_prod[threadIdx.x]);
   }
-  if (threadIdx.x == 0 && s_words) atomicAdd(&ctr->sym_words, s_words);
+  if (threadIdx.x == 32) {
+    if (s_words) atomicAdd(&ctr->sym_words, s_words);
+    if (s_tot) atomicAdd(&ctr->total_products, s_tot);
+    if (s_maxp) atomicMax(&ctr->max_products, s_maxp);
+    if (s_maxa) atomicMax(&ctr->max_a_nnz, s_maxa);
+  }
+}
+
+// The analysis of the listed long rows: the warps of the grid stride over the
+// chunk ids, merge each chunk's partial sums into its row's accumulator with
+// atomics, and the warp that finishes a row's last chunk writes the row's
+// results, appends it to its class and adds its totals.
+template <typename RP>
+__global__ void __launch_bounds__(256) k_analysis_long(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
+                                                       uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
+                                                       uint32_t* __restrict__ anz, uint32_t* __restrict__ maxb,
+                                                       uint32_t* __restrict__ row_nnz,
+                                                       uint64_t* __restrict__ bm_off, uint32_t* __restrict__ sym_bins,
+                                                       DevCounters* __restrict__ ctr, SymPolicySet pols,
+                                                       const uint8_t* __restrict__ row_pol,
+                                                       const uint32_t* __restrict__ long_rows,
+                                                       LongRowAcc* __restrict__ long_acc, uint32_t long_cap,
+                                                       const uint32_t* __restrict__ long_chunk_row,
+                                                       uint32_t chunk_cap) {
+  const uint32_t total = min(ctr->long_chunks, chunk_cap);
+  const uint32_t nl = min(ctr->num_long, long_cap);
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < total; c += nw) {
+    const uint32_t i = long_chunk_row[c];
+    if (i >= nl) continue;  // (a row that did not fit the map: flagged by the analysis)
+    LongRowAcc& L = long_acc[i];
+    const uint32_t row = long_rows[i];
+    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+    const uint32_t nch = (uint32_t)((a1 - a0 + kLongChunk - 1) / kLongChunk);
+    if (c - L.base >= nch) continue;
+    const uint64_t c0 = a0 + (uint64_t)(c - L.base) * kLongChunk;
+    unsigned long long p = 0;
+    uint32_t mn = kEmpty, mx = 0, lb = 0;
+    span_part<32>(A, B, c0 + lane, min(a1, c0 + kLongChunk), p, mn, mx, lb);
+    p = warp_sum_u64(p);
+    mn = __reduce_min_sync(kFull, mn);
+    mx = __reduce_max_sync(kFull, mx);
+    lb = __reduce_max_sync(kFull, lb);
+    if (lane == 0) {
+      if (p) atomicAdd(&L.prod, p);
+      atomicMin(&L.lo, mn);
+      atomicMax(&L.hi, mx);
+      atomicMax(&L.maxb, lb);
+      __threadfence();
+      if (atomicAdd(&L.done, 1u) == nch - 1) {
+        __threadfence();
+        const unsigned long long tp = atomicAdd(&L.prod, 0ull);
+        const uint32_t tmn = atomicOr(&L.lo, 0u), tmx = atomicOr(&L.hi, 0u), tlb = atomicOr(&L.maxb, 0u);
+        const int b = analysis_write(row, a1 - a0, tp, tmn, tmx, tlb, prod, lo, hi, anz, maxb, row_nnz, bm_off,
+                                     pols, row_pol);
+        if (b >= 0) {
+          const unsigned pos = atomicAdd(&ctr->sym_count[b], 1u);
+          sym_bins[(uint64_t)b * A.rows + pos] = row;
+          atomicAdd(&ctr->sym_anz[b], (unsigned long long)(a1 - a0));
+          atomicAdd(&ctr->sym_prod[b], tp);
+          const uint64_t span = (uint64_t)tmx - tmn + 1;
+          if (b == SB_BITMAP && span <= kBitmapBits) atomicAdd(&ctr->sym_words, (unsigned long long)((span + 63) >> 6));
+          atomicAdd(&ctr->total_products, tp);
+          atomicMax(&ctr->max_products, tp > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned)tp);
+        }
+      }
+    }
+    __syncwarp();
+  }
 }
 
 // ---------------------------------------------------------------- ESC (<= 32K products)
 // Expand-sort-compress in the registers of one warp: a row's (<= 32K)
-// products are listed, held K per lane (element i = e*32 + lane lives in
-// register e of lane i%32), bitonic-sorted by column across the warp (shuffles
-// for partners in other lanes, register swaps for partners in the same lane),
-// then equal columns are merged by a segmented suffix sum that carries across
-// register rows. The output is the row, sorted, with no shared-memory table and
-// no block barrier. The symbolic variant sorts keys only and counts run heads.
+// products are listed, held K per lane, bitonic-sorted by column across the
+// warp into blocked order (lane l ends with sorted elements l*K .. l*K+K-1;
+// register swaps for partners in the same lane, shuffles for the others), then
+// equal columns are merged by suffix sums inside each lane and one segmented
+// scan across lanes. The output is the row, sorted, with no shared-memory
+// table and no block barrier. The symbolic variant sorts keys only and counts
+// run heads.
 
 // Lists the (<= CAP) products of `row` in warp order: src[i] = index into B,
 // aidx[i] = index into A. Returns the product count (> CAP means overflow).
@@ -272,46 +421,61 @@ __device__ __forceinline__ uint32_t gather_products(const Csr<RP>& A, const Csr<
   return base;
 }
 
-// Bitonic sort of the warp's 32K (key, value) elements, ascending by key.
+// Bitonic sort of the warp's 32K (key, value) elements into blocked order:
+// afterwards lane l holds sorted elements l*K .. l*K + K - 1 in registers
+// 0 .. K - 1 (element L = lane*K + e). Stages whose partner element lies in
+// the same lane (j < K) swap registers; the others exchange one register with
+// lane ^ (j / K). Against the strided layout this moves log2(K) stages of
+// every merge into registers and lets the merge that follows scan each lane's
+// run locally before one scan across lanes.
 template <int K, bool VALS>
-__device__ __forceinline__ void warp_bitonic_sort(uint32_t (&key)[K], double (&val)[K]) {
+__device__ __forceinline__ void warp_sort_blocked(uint32_t (&key)[K], double (&val)[K]) {
   const int lane = threadIdx.x & 31;
   constexpr int N = 32 * K;
 #pragma unroll
   for (int k = 2; k <= N; k <<= 1) {
 #pragma unroll
     for (int j = k >> 1; j > 0; j >>= 1) {
-      if (j >= 32) {
-        const int je = j >> 5;
+      if (j < K) {
 #pragma unroll
         for (int e = 0; e < K; ++e) {
-          if ((e & je) == 0) {
-            const int e2 = e | je;
-            const bool asc = (((e << 5) | lane) & k) == 0;
-            if ((key[e] > key[e2]) == asc) {
+          if ((e & j) == 0) {
+            const int e2 = e | j;
+            const bool asc = ((lane * K + e) & k) == 0;
+            if (!VALS) {
+              const uint32_t a = key[e], b = key[e2];
+              key[e] = asc ? min(a, b) : max(a, b);
+              key[e2] = asc ? max(a, b) : min(a, b);
+            } else if ((key[e] > key[e2]) == asc) {
               const uint32_t tk = key[e];
               key[e] = key[e2];
               key[e2] = tk;
-              if (VALS) {
-                const double tv = val[e];
-                val[e] = val[e2];
-                val[e2] = tv;
-              }
+              const double tv = val[e];
+              val[e] = val[e2];
+              val[e2] = tv;
             }
           }
         }
       } else {
+        const int lj = j / K;
+        const bool asc = ((lane * K) & k) == 0;  // k > j >= K: the register index does not reach bit k
+        const bool low = (lane & lj) == 0;
+        const bool keep_min = low == asc;  // this lane keeps the smaller key of the pair
 #pragma unroll
         for (int e = 0; e < K; ++e) {
-          const uint32_t ok = __shfl_xor_sync(kFull, key[e], j);
-          double ov = 0.0;
-          if (VALS) ov = __shfl_xor_sync(kFull, val[e], j);
-          const bool asc = (((e << 5) | lane) & k) == 0;
-          const bool low = (lane & j) == 0;
-          const bool take = (low == asc) ? (ok < key[e]) : (ok > key[e]);
-          if (take) {
-            key[e] = ok;
-            if (VALS) val[e] = ov;
+          const uint32_t ok = __shfl_xor_sync(kFull, key[e], lj);
+          if (!VALS) {
+            // keys only: one predicated min/max per element (equal keys are
+            // interchangeable)
+            key[e] = keep_min ? min(key[e], ok) : max(key[e], ok);
+          } else {
+            // with values the strict test keeps both lanes of a tie on their
+            // own element
+            const double ov = __shfl_xor_sync(kFull, val[e], lj);
+            if (keep_min ? (ok < key[e]) : (ok > key[e])) {
+              key[e] = ok;
+              val[e] = ov;
+            }
           }
         }
       }
@@ -319,19 +483,56 @@ __device__ __forceinline__ void warp_bitonic_sort(uint32_t (&key)[K], double (&v
   }
 }
 
-// Run heads of the sorted keys: head if the key is real and differs from the
-// previous element in sort order. hb[e] = ballot of heads in register row e.
+// Run heads of blocked-sorted keys (kEmpty last): head[e] if the key is real
+// and differs from the element before it. Returns the warp's number of runs;
+// `before` = runs that start in lanes below this one.
 template <int K>
-__device__ __forceinline__ void warp_run_heads(const uint32_t (&key)[K], unsigned (&hb)[K], bool (&head)[K]) {
+__device__ __forceinline__ uint32_t warp_heads_blocked(const uint32_t (&key)[K], bool (&head)[K],
+                                                       uint32_t& before) {
   const int lane = threadIdx.x & 31;
+  const uint32_t prev_last = __shfl_up_sync(kFull, key[K - 1], 1);
+  const unsigned lt = lanemask_lt();
+  uint32_t n = 0;
+  before = 0;
 #pragma unroll
   for (int e = 0; e < K; ++e) {
-    const uint32_t up = __shfl_up_sync(kFull, key[e], 1);
-    uint32_t prev_last = kEmpty;
-    if (e > 0) prev_last = __shfl_sync(kFull, key[e - 1], 31);
-    const uint32_t prev = lane > 0 ? up : prev_last;
-    head[e] = key[e] != kEmpty && (((e << 5) | lane) == 0 || prev != key[e]);
-    hb[e] = __ballot_sync(kFull, head[e]);
+    const uint32_t prev = e > 0 ? key[e - 1] : prev_last;
+    head[e] = key[e] != kEmpty && ((e == 0 && lane == 0) || prev != key[e]);
+    const unsigned hb = __ballot_sync(kFull, head[e]);
+    n += __popc(hb);
+    before += __popc(hb & lt);
+  }
+  return n;
+}
+
+// Segmented sums of blocked-sorted (key, val): afterwards the first element
+// of every run of equal keys holds the run's sum. Suffix sums inside each
+// lane, then one segmented suffix scan across lanes of each lane's first-run
+// sum (keys are sorted, so a lane whose first key equals a later lane's first
+// key holds that key only, and key equality alone delimits the segments),
+// then the lane's last run takes the sum of its continuation in the lanes
+// above.
+template <int K>
+__device__ __forceinline__ void warp_merge_blocked(const uint32_t (&key)[K], double (&val)[K]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int e = K - 2; e >= 0; --e)
+    if (key[e] == key[e + 1]) val[e] += val[e + 1];
+  const uint32_t kf = key[0];
+  double acc = val[0];
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t ck = __shfl_down_sync(kFull, kf, d);
+    const double cv = __shfl_down_sync(kFull, acc, d);
+    if (lane + d < 32 && ck == kf) acc += cv;
+  }
+  const uint32_t nk = __shfl_down_sync(kFull, kf, 1);
+  const double nacc = __shfl_down_sync(kFull, acc, 1);
+  const uint32_t kl = key[K - 1];
+  if (lane < 31 && nk == kl) {
+#pragma unroll
+    for (int e = 0; e < K; ++e)
+      if (key[e] == kl) val[e] += nacc;
   }
 }
 
@@ -362,13 +563,10 @@ __global__ void __launch_bounds__(256) k_sym_esc(Csr<RP> A, Csr<RP> B, RowQueue 
       const bool first = key[0] != kEmpty && (__ffs(peers) - 1 == lane);
       n = __popc(__ballot_sync(kFull, first));
     } else {
-      warp_bitonic_sort<K, false>(key, val);
-      unsigned hb[K];
+      warp_sort_blocked<K, false>(key, val);
       bool head[K];
-      warp_run_heads<K>(key, hb, head);
-      n = 0;
-#pragma unroll
-      for (int e = 0; e < K; ++e) n += __popc(hb[e]);
+      uint32_t before;
+      n = warp_heads_blocked<K>(key, head, before);
     }
     if (lane == 0) row_nnz[row] = n;
     __syncwarp();
@@ -425,7 +623,7 @@ __global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, RowQueue 
         pk[e] = key[e] == kEmpty ? kEmpty : ((key[e] - kmin) << LOGN) | pos;
       }
       __syncwarp();
-      warp_bitonic_sort<K, false>(pk, val);
+      warp_sort_blocked<K, false>(pk, val);
 #pragma unroll
       for (int e = 0; e < K; ++e) {
         if (pk[e] == kEmpty) {
@@ -438,49 +636,26 @@ __global__ void __launch_bounds__(256) k_num_esc(Csr<RP> A, Csr<RP> B, RowQueue 
       }
       __syncwarp();
     } else {
-      warp_bitonic_sort<K, true>(key, val);
+      warp_sort_blocked<K, true>(key, val);
     }
-    // segmented suffix sums inside each register row
-#pragma unroll
-    for (int e = 0; e < K; ++e) {
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t ck = __shfl_down_sync(kFull, key[e], d);
-        const double cv = __shfl_down_sync(kFull, val[e], d);
-        if (lane + d < 32 && ck == key[e]) val[e] += cv;
-      }
-    }
-    // carry runs that continue into the next register row, last row first
-    uint32_t carry_key = kEmpty;
-    double carry = 0.0;
-#pragma unroll
-    for (int e = K - 1; e >= 0; --e) {
-      const uint32_t last = __shfl_sync(kFull, key[e], 31);
-      if (key[e] == last && last == carry_key && last != kEmpty) val[e] += carry;
-      carry_key = __shfl_sync(kFull, key[e], 0);
-      carry = __shfl_sync(kFull, val[e], 0);
-    }
-    unsigned hb[K];
+    // lane l now holds sorted elements l*K .. l*K + K - 1: run sums, heads
+    warp_merge_blocked<K>(key, val);
     bool head[K];
-    warp_run_heads<K>(key, hb, head);
-    uint32_t n = 0;
-#pragma unroll
-    for (int e = 0; e < K; ++e) n += __popc(hb[e]);
+    uint32_t before;
+    const uint32_t n = warp_heads_blocked<K>(key, head, before);
     const uint32_t cap = o.cap[row];
     int accept = 0;
     if (lane == 0) accept = out_accept(o, ctr, row, n, cap);
     accept = __shfl_sync(kFull, accept, 0);
     const uint32_t lim = accept ? min(n, cap) : 0u;
     const uint64_t off = o.off[row];
-    uint32_t before = 0;
 #pragma unroll
     for (int e = 0; e < K; ++e) {
-      const uint32_t pos = before + __popc(hb[e] & lanemask_lt());
-      if (head[e] && pos < lim) {
-        c_col[off + pos] = key[e];
-        c_val[off + pos] = val[e];
+      if (head[e] && before < lim) {
+        c_col[off + before] = key[e];
+        c_val[off + before] = val[e];
       }
-      before += __popc(hb[e]);
+      before += head[e] ? 1u : 0u;
     }
     __syncwarp();
   }
@@ -515,46 +690,26 @@ struct UspSmem {
   uint32_t tile;
 };
 
-// Segmented sums of the sorted (key, val) of one row (kEmpty keys last), then
-// the distinct columns and their sums written compactly to okey/oval.
-// Returns the row's output count. Warp-collective.
+// Segmented sums of the blocked-sorted (key, val) of one row (kEmpty keys
+// last), then the distinct columns and their sums written compactly to
+// okey/oval. Returns the row's output count. Warp-collective.
 template <int K>
 __device__ __forceinline__ uint32_t usp_merge_stage(uint32_t (&key)[K], double (&val)[K], uint32_t* okey,
                                                     double* oval) {
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int e = 0; e < K; ++e) {
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t ck = __shfl_down_sync(kFull, key[e], d);
-      const double cv = __shfl_down_sync(kFull, val[e], d);
-      if (lane + d < 32 && ck == key[e]) val[e] += cv;
-    }
-  }
-  uint32_t carry_key = kEmpty;
-  double carry = 0.0;
-#pragma unroll
-  for (int e = K - 1; e >= 0; --e) {
-    const uint32_t last = __shfl_sync(kFull, key[e], 31);
-    if (key[e] == last && last == carry_key && last != kEmpty) val[e] += carry;
-    carry_key = __shfl_sync(kFull, key[e], 0);
-    carry = __shfl_sync(kFull, val[e], 0);
-  }
-  unsigned hb[K];
+  warp_merge_blocked<K>(key, val);
   bool head[K];
-  warp_run_heads<K>(key, hb, head);
-  uint32_t before = 0;
+  uint32_t before;
+  const uint32_t n = warp_heads_blocked<K>(key, head, before);
 #pragma unroll
   for (int e = 0; e < K; ++e) {
     if (head[e]) {
-      const uint32_t pos = before + __popc(hb[e] & lanemask_lt());
-      okey[pos] = key[e];
-      oval[pos] = val[e];
+      okey[before] = key[e];
+      oval[before] = val[e];
+      ++before;
     }
-    before += __popc(hb[e]);
   }
   __syncwarp();
-  return before;
+  return n;
 }
 
 // Register ESC of a row of np <= 32K products gathered in src/aidx; the
@@ -595,7 +750,7 @@ __device__ __forceinline__ uint32_t usp_row_regs(const Csr<RP>& A, const Csr<RP>
       pk[e] = key[e] == kEmpty ? kEmpty : ((key[e] - kmin) << LOGN) | pos;
     }
     __syncwarp();
-    warp_bitonic_sort<K, false>(pk, val);
+    warp_sort_blocked<K, false>(pk, val);
 #pragma unroll
     for (int e = 0; e < K; ++e) {
       if (pk[e] == kEmpty) {
@@ -608,7 +763,7 @@ __device__ __forceinline__ uint32_t usp_row_regs(const Csr<RP>& A, const Csr<RP>
     }
     __syncwarp();
   } else {
-    warp_bitonic_sort<K, true>(key, val);
+    warp_sort_blocked<K, true>(key, val);
   }
   return usp_merge_stage<K>(key, val, okey, oval);
 }
@@ -648,7 +803,7 @@ __device__ __forceinline__ uint32_t usp_row_smem(const Csr<RP>& A, const Csr<RP>
   double val[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
-    const uint64_t kk = src[(e << 5) | lane];
+    const uint64_t kk = src[(lane << 3) | e];  // blocked order: lane l takes sorted elements 8l .. 8l + 7
     key[e] = kk == ~0ull ? kEmpty : (uint32_t)(kk >> 8);
     val[e] = kk == ~0ull ? 0.0 : oval[kk & 255];
   }
@@ -1910,7 +2065,9 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
                                                      const uint8_t* __restrict__ row_pol, int bin_rows) {
   __shared__ unsigned long long scr[33];
   __shared__ unsigned long long s_cls[3][NB_COUNT];
+  __shared__ unsigned s_cnt[NB_COUNT];
   if (threadIdx.x < 3 * NB_COUNT) (&s_cls[0][0])[threadIdx.x] = 0ull;
+  if (threadIdx.x < NB_COUNT) s_cnt[threadIdx.x] = 0u;
   const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * 4;
   uint32_t v[4];
   unsigned long long s = 0;
@@ -1921,8 +2078,8 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
   }
   unsigned long long total;
   unsigned long long run = block_excl_scan<1024, unsigned long long>(s, scr, &total) + tile_offs[blockIdx.x];
-  // per-class sums of this thread's rows (nnz, A entries, products)
-  unsigned long long my_nnz[NB_COUNT] = {0}, my_anz[NB_COUNT] = {0}, my_prod[NB_COUNT] = {0};
+  int bq[4];
+  uint32_t rq[4], aq[4], pq[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const uint64_t i = base + q;
@@ -1938,25 +2095,36 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
       b = num_bin_for(v[q], p, (uint64_t)hi[i] - lo[i] + 1, pol);
       if (b >= 0 && pol.force_bin < 0 && bm_off[i] != ~0ull) b = NB_BITMAP;  // reuse the saved bitmap
       if (b == NB_BITMAP && (uint64_t)hi[i] - lo[i] + 1 > kBitmapBits) atomicAdd(&ctr->num_wide, 1u);
-#pragma unroll
-      for (int c = 0; c < NB_COUNT; ++c) {
-        if (b == c) {
-          my_nnz[c] += v[q];
-          my_anz[c] += anz[i];
-          my_prod[c] += p;
-        }
-      }
+      aq[q] = anz[i];
+      pq[q] = p;
     }
-    if (bin_rows) bin_append(b, (uint32_t)i, ctr->num_count, num_bins, n);
+    bq[q] = b;
+    rq[q] = (uint32_t)i;
   }
   if (!bin_rows) return;
-  // warp sums first, then one shared atomic per warp and class
+  block_bin_append<4>(bq, rq, s_cnt, NB_COUNT, ctr->num_count, num_bins, n);
+  // per-class sums (nnz, A entries, products) of the classes present in the
+  // warp: warp sums, then one shared atomic per warp and class
   const int lane = threadIdx.x & 31;
+  unsigned present = 0;
 #pragma unroll
-  for (int c = 0; c < NB_COUNT; ++c) {
-    const unsigned long long a = warp_sum_u64(my_nnz[c]);
-    const unsigned long long b2 = warp_sum_u64(my_anz[c]);
-    const unsigned long long d = warp_sum_u64(my_prod[c]);
+  for (int q = 0; q < 4; ++q) present |= bq[q] >= 0 ? 1u << bq[q] : 0u;
+  present = __reduce_or_sync(kFull, present);
+  while (present) {
+    const int c = __ffs(present) - 1;
+    present &= present - 1;
+    unsigned long long a = 0, b2 = 0, d = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (bq[q] == c) {
+        a += v[q];
+        b2 += aq[q];
+        d += pq[q];
+      }
+    }
+    a = warp_sum_u64(a);
+    b2 = warp_sum_u64(b2);
+    d = warp_sum_u64(d);
     if (lane == 0 && a) {
       atomicAdd(&s_cls[0][c], a);
       atomicAdd(&s_cls[1][c], b2);
@@ -2028,23 +2196,38 @@ __global__ void __launch_bounds__(256) k_hll_sketch(Csr<RP> B, uint8_t* __restri
   }
 }
 
-// Raw HLL estimate of the output size of A row `row` (warp-collective; every
-// lane gets the result). Lane l merges word (l % W) of the sketches of every
-// (32 / W)-th A entry with a packed per-byte maximum; xor shuffles finish the
-// union; the harmonic sum runs over the lanes that own a word.
+// HLL sketch union over A entries [k0, k1) (warp-collective): lane l merges
+// word (l % W) of the sketches of every (32 / W)-th entry with a packed
+// per-byte maximum, four entries' loads in flight per pass. The lane's word
+// is returned unreduced across the lanes that share it.
 template <typename RP, int LOGP>
-__device__ __forceinline__ int hll_row_estimate(const Csr<RP>& A, const uint8_t* __restrict__ sk, uint64_t row) {
+__device__ __forceinline__ unsigned hll_merge_part(const Csr<RP>& A, const uint8_t* __restrict__ sk, uint64_t k0,
+                                                   uint64_t k1) {
   constexpr int M = 1 << LOGP;
-  constexpr int W = M / 4;       // 32-bit words per sketch
-  constexpr int G = 32 / W;      // A entries merged per step
+  constexpr int W = M / 4;   // 32-bit words per sketch
+  constexpr int G = 32 / W;  // A entries merged per step
+  const int lane = threadIdx.x & 31;
+  unsigned acc = 0u;
+  for (uint64_t k = k0 + lane / W; k < k1; k += 4 * G) {
+    uint32_t j[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) j[u] = k + (uint64_t)u * G < k1 ? A.col[k + (uint64_t)u * G] : kEmpty;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (j[u] != kEmpty) acc = __vmaxu4(acc, reinterpret_cast<const unsigned*>(sk + (uint64_t)j[u] * M)[lane % W]);
+  }
+  return acc;
+}
+
+// Raw HLL estimate from the lanes' words (warp-collective; every lane gets the
+// result): xor shuffles finish the union, the harmonic sum runs over the lanes
+// that own a word, with the small-range correction.
+template <int LOGP>
+__device__ __forceinline__ int hll_finish(unsigned acc) {
+  constexpr int M = 1 << LOGP;
+  constexpr int W = M / 4;
   constexpr double kAlpha = LOGP == 4 ? 0.673 : (LOGP == 5 ? 0.697 : (LOGP == 6 ? 0.709 : 0.715));
   const int lane = threadIdx.x & 31;
-  const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
-  unsigned acc = 0u;
-  for (uint64_t k = a0 + lane / W; k < a1; k += G) {
-    const uint32_t j = A.col[k];
-    acc = __vmaxu4(acc, reinterpret_cast<const unsigned*>(sk + (uint64_t)j * M)[lane % W]);
-  }
 #pragma unroll
   for (int o = W; o < 32; o <<= 1) acc = __vmaxu4(acc, __shfl_xor_sync(kFull, acc, o));
   double z = 0.0;
@@ -2067,36 +2250,114 @@ __device__ __forceinline__ int hll_row_estimate(const Csr<RP>& A, const uint8_t*
   return result;
 }
 
+// Raw HLL estimate of the output size of A row `row` (warp-collective; every
+// lane gets the result).
+template <typename RP, int LOGP>
+__device__ __forceinline__ int hll_row_estimate(const Csr<RP>& A, const uint8_t* __restrict__ sk, uint64_t row) {
+  return hll_finish<LOGP>(hll_merge_part<RP, LOGP>(A, sk, A.row_begin(row), A.row_end(row)));
+}
+
+// A row's sizing value from its raw HLL estimate: raw_only, the raw value;
+// otherwise raw x expansion, at least 1 and at most min(products, column span).
+__device__ __forceinline__ uint32_t hll_value(int raw, uint32_t p, uint32_t lo, uint32_t hi, double expansion,
+                                              int raw_only) {
+  if (raw_only) return raw > 0 ? (uint32_t)raw : 0u;
+  const uint64_t span = (uint64_t)hi - lo + 1;
+  double e = ceil((double)raw * expansion);
+  if (e < 1.0) e = 1.0;
+  uint64_t v = (uint64_t)e;
+  v = v < p ? v : p;
+  v = v < span ? v : span;
+  return (uint32_t)v;
+}
+
 // Estimated output count of every A row for the estimation workflow: rows of at
 // most esc_max products get their product count (an exact upper bound, they run
 // in the register classes); others the HLL estimate times `expansion`, at least
-// 1 and at most min(products, column span).
+// 1 and at most min(products, column span), or (raw_only) the raw HLL
+// estimate. Rows that the analysis listed as long (long_acc set) are left to
+// k_hll_estimate_long.
 template <typename RP, int LOGP>
 __global__ void __launch_bounds__(256) k_hll_estimate(Csr<RP> A, const uint8_t* __restrict__ sk,
                                                       const uint32_t* __restrict__ prod,
                                                       const uint32_t* __restrict__ lo,
                                                       const uint32_t* __restrict__ hi, uint32_t* __restrict__ est,
-                                                      double expansion, uint32_t esc_max, int raw_only) {
+                                                      double expansion, uint32_t esc_max, int raw_only,
+                                                      const LongRowAcc* __restrict__ long_acc) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint64_t r = (uint64_t)blockIdx.x * 8 + warp; r < A.rows; r += (uint64_t)gridDim.x * 8) {
     const uint32_t p = prod[r];
-    if (!raw_only && p <= esc_max) {  // warp-uniform
+    if (p <= esc_max) {  // warp-uniform
       if (lane == 0) est[r] = p;
       continue;
     }
+    if (long_acc && A.row_end(r) - A.row_begin(r) > kLongRowEntries) continue;
     const int raw = hll_row_estimate<RP, LOGP>(A, sk, r);
-    if (raw_only) {
-      if (lane == 0) est[r] = raw > 0 ? (uint32_t)raw : 0u;
-      continue;
+    if (lane == 0) est[r] = hll_value(raw, p, lo[r], hi[r], expansion, raw_only);
+  }
+}
+
+// HLL estimates of the listed long rows: the warps of the grid stride over
+// the chunk ids (as in k_analysis_long), merge each chunk's union into the
+// row's registers with per-register atomicMax, and the warp that finishes the
+// row's last chunk computes the row's estimate.
+template <typename RP, int LOGP>
+__global__ void __launch_bounds__(256) k_hll_estimate_long(Csr<RP> A, const uint8_t* __restrict__ sk,
+                                                           const uint32_t* __restrict__ prod,
+                                                           const uint32_t* __restrict__ lo,
+                                                           const uint32_t* __restrict__ hi,
+                                                           uint32_t* __restrict__ est, double expansion,
+                                                           uint32_t esc_max, int raw_only,
+                                                           const DevCounters* __restrict__ ctr,
+                                                           const uint32_t* __restrict__ long_rows,
+                                                           LongRowAcc* __restrict__ long_acc, uint32_t long_cap,
+                                                           const uint32_t* __restrict__ long_chunk_row,
+                                                           uint32_t chunk_cap) {
+  constexpr int W = (1 << LOGP) / 4;
+  const uint32_t total = min(ctr->long_chunks, chunk_cap);
+  const uint32_t nl = min(ctr->num_long, long_cap);
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < total; c += nw) {
+    const uint32_t i = long_chunk_row[c];
+    if (i >= nl) continue;  // (a row that did not fit the map: flagged by the analysis)
+    LongRowAcc& L = long_acc[i];
+    const uint32_t row = long_rows[i];
+    const uint32_t p = prod[row];
+    if (p <= esc_max) continue;  // sized by k_hll_estimate
+    const uint64_t a0 = A.row_begin(row), a1 = A.row_end(row);
+    const uint32_t nch = (uint32_t)((a1 - a0 + kLongChunk - 1) / kLongChunk);
+    if (c - L.base >= nch) continue;
+    const uint64_t c0 = a0 + (uint64_t)(c - L.base) * kLongChunk;
+    unsigned acc = hll_merge_part<RP, LOGP>(A, sk, c0, min(a1, c0 + kLongChunk));
+#pragma unroll
+    for (int o = W; o < 32; o <<= 1) acc = __vmaxu4(acc, __shfl_xor_sync(kFull, acc, o));
+    if (lane < W) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const unsigned v = (acc >> (8 * b)) & 0xFFu;
+        if (v) atomicMax(&L.reg[lane * 4 + b], v);
+      }
     }
-    if (lane == 0) {
-      const uint64_t span = (uint64_t)hi[r] - lo[r] + 1;
-      double e = ceil((double)raw * expansion);
-      if (e < 1.0) e = 1.0;
-      uint64_t v = (uint64_t)e;
-      v = v < p ? v : p;
-      v = v < span ? v : span;
-      est[r] = (uint32_t)v;
+    __threadfence();
+    __syncwarp();
+    unsigned last = 0;
+    if (lane == 0) last = atomicAdd(&L.hdone, 1u) == nch - 1;
+    last = __shfl_sync(kFull, last, 0);
+    if (last) {
+      // every chunk of the row is merged: read the registers and leave them
+      // (and the counter) zeroed for a later estimate after the same analysis
+      __threadfence();
+      unsigned word = 0u;
+      if (lane < W) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) word |= (atomicExch(&L.reg[lane * 4 + b], 0u) & 0xFFu) << (8 * b);
+      }
+      const int raw = hll_finish<LOGP>(word);
+      if (lane == 0) {
+        est[row] = hll_value(raw, p, lo[row], hi[row], expansion, raw_only);
+        atomicExch(&L.hdone, 0u);
+      }
     }
   }
 }
@@ -2127,7 +2388,12 @@ __global__ void __launch_bounds__(256) k_hll_sample(Csr<RP> A, const uint8_t* __
 }
 
 // Estimation-workflow epilogue: rows that fit their estimate are copied from
-// the temporary output (slots at src_off) to C (dst_off), one warp per row.
+// the temporary output (slots at src_off) to C (dst_off). A block takes 256
+// consecutive rows, scans their counts and deals the tile's entries out to its
+// threads in order, each finding its row by a search of the tile's inclusive
+// offsets in shared memory: loads and stores stay coalesced across row ends
+// and the work per thread does not depend on the row lengths (rows of a few
+// dozen entries left most lanes of a warp-per-row copy idle).
 __global__ void __launch_bounds__(256) k_copy_rows(uint64_t rows, const uint64_t* __restrict__ src_off,
                                                    const uint32_t* __restrict__ cap,
                                                    const uint32_t* __restrict__ cnt,
@@ -2136,15 +2402,37 @@ __global__ void __launch_bounds__(256) k_copy_rows(uint64_t rows, const uint64_t
                                                    const double* __restrict__ t_val, uint32_t* __restrict__ c_col,
                                                    double* __restrict__ c_val, const unsigned* __restrict__ stop) {
   if (stop && (*stop & DEV_BATCH_MISMATCH)) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint64_t r = (uint64_t)blockIdx.x * 8 + warp; r < rows; r += (uint64_t)gridDim.x * 8) {
-    const uint32_t n = cnt[r];
-    if (n == 0 || n == kUnknownCount || n > cap[r]) continue;
-    const uint64_t s0 = src_off[r], d0 = dst_off[r];
-    for (uint32_t i = lane; i < n; i += 32) {
-      c_col[d0 + i] = t_col[s0 + i];
-      c_val[d0 + i] = t_val[s0 + i];
+  __shared__ unsigned long long s_incl[256];
+  __shared__ uint64_t s_src[256], s_dst[256];
+  __shared__ unsigned long long scr[33];
+  const int tid = threadIdx.x;
+  for (uint64_t r0 = (uint64_t)blockIdx.x * 256; r0 < rows; r0 += (uint64_t)gridDim.x * 256) {
+    const uint64_t r = r0 + tid;
+    uint32_t n = 0;
+    if (r < rows) {
+      n = cnt[r];
+      if (n == kUnknownCount || n > cap[r]) n = 0;
     }
+    s_src[tid] = n ? src_off[r] : 0ull;
+    s_dst[tid] = n ? dst_off[r] : 0ull;
+    unsigned long long total;
+    const unsigned long long ex = block_excl_scan<256, unsigned long long>(n, scr, &total);
+    s_incl[tid] = ex + n;
+    __syncthreads();
+    int t = 0;  // row of the previous entry: entries ascend, so rows do too
+    for (unsigned long long e = tid; e < total; e += 256) {
+      int lo = t, hi = 255;  // first row whose inclusive offset exceeds e
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (s_incl[mid] <= e) lo = mid + 1;
+        else hi = mid;
+      }
+      t = lo;
+      const unsigned long long k = e - (t ? s_incl[t - 1] : 0ull);
+      c_col[s_dst[t] + k] = t_col[s_src[t] + k];
+      c_val[s_dst[t] + k] = t_val[s_src[t] + k];
+    }
+    __syncthreads();
   }
 }
 
@@ -2245,15 +2533,27 @@ int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const 
   SymPolicySet pols;
   for (int i = 0; i < kPolicySlots; ++i) pols.p[i] = (i > 0 && seg) ? seg[i - 1] : pol;
   const uint8_t* row_pol = seg ? w.row_pol : nullptr;
+  // lanes per row: the smallest power of two (at least 4) whose pass of 4
+  // entries per lane covers the mean row length; one row per 4 lanes measured
+  // fastest on short rows (fewer threads, less per-row overhead)
   const double avg = (double)A.nnz / (double)A.rows;
-  if (avg >= 12.0) {
-    const uint64_t threads = A.rows * 32;
-    k_analysis<RP, 32><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pols, row_pol);
-  } else {
-    const uint64_t threads = A.rows * 4;
-    k_analysis<RP, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-        A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, w.ctr, pols, row_pol);
+  const int g = avg <= 16.0 ? 4 : avg <= 32.0 ? 8 : avg <= 64.0 ? 16 : 32;
+  const uint64_t per_block = 256 / g;
+  const unsigned blocks = (unsigned)((A.rows + per_block - 1) / per_block);
+#define OCEAN_ANALYSIS(G)                                                                                          \
+  k_analysis<RP, G><<<blocks, 256, 0, s>>>(A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, \
+                                           w.ctr, pols, row_pol, w.long_rows, w.long_acc, w.long_cap, w.long_chunk_row, \
+                                           w.long_chunk_cap)
+  if (g == 32) OCEAN_ANALYSIS(32);
+  else if (g == 16) OCEAN_ANALYSIS(16);
+  else if (g == 8) OCEAN_ANALYSIS(8);
+  else OCEAN_ANALYSIS(4);
+#undef OCEAN_ANALYSIS
+  if (w.long_acc) {
+    k_analysis_long<RP><<<4 * 148, 256, 0, s>>>(A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off,
+                                                w.sym_bins, w.ctr, pols, row_pol, w.long_rows, w.long_acc, w.long_cap,
+                                                w.long_chunk_row, w.long_chunk_cap);
+    return 2;
   }
   return 1;
 }
@@ -2434,17 +2734,27 @@ int launch_hll_rows(const Csr<RP>& A, const DevWork& w, int log2p, double expans
                     const uint8_t* sketch, uint32_t* out, cudaStream_t s) {
   if (A.rows == 0) return 0;
   const unsigned ga = (unsigned)std::min<uint64_t>((A.rows + 7) / 8, 65535u * 8);
+  const int ro = raw ? 1 : 0;
   if (log2p == 5)
-    k_hll_estimate<RP, 5><<<ga, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, raw ? 1 : 0);
+    k_hll_estimate<RP, 5><<<ga, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro, w.long_acc);
   else
-    k_hll_estimate<RP, 6><<<ga, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, raw ? 1 : 0);
-  return 1;
+    k_hll_estimate<RP, 6><<<ga, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro, w.long_acc);
+  if (!w.long_acc) return 1;
+  if (log2p == 5)
+    k_hll_estimate_long<RP, 5><<<4 * 148, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro,
+                                                       w.ctr, w.long_rows, w.long_acc, w.long_cap,
+                                                       w.long_chunk_row, w.long_chunk_cap);
+  else
+    k_hll_estimate_long<RP, 6><<<4 * 148, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro,
+                                                       w.ctr, w.long_rows, w.long_acc, w.long_cap,
+                                                       w.long_chunk_row, w.long_chunk_cap);
+  return 2;
 }
 
 void launch_copy_rows(const DevWork& w, const uint32_t* t_col, const double* t_val, uint32_t* c_col, double* c_val,
                       cudaStream_t s, const unsigned* stop) {
   if (w.rows == 0) return;
-  const unsigned g = (unsigned)std::min<uint64_t>((w.rows + 7) / 8, 148u * 64u);
+  const unsigned g = (unsigned)std::min<uint64_t>((w.rows + 255) / 256, 148u * 8u);
   k_copy_rows<<<g, 256, 0, s>>>(w.rows, w.est_off, w.est, w.cnt, w.rowptr64, t_col, t_val, c_col, c_val, stop);
 }
 

@@ -212,7 +212,9 @@ struct ocean_handle {
   void free_all() {
     DevWork& x = w;
     void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.maxb, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
-                  x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf, x.ctr, wide_a, wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
+                  x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf, x.long_rows, x.long_acc, x.long_chunk_row,
+                  x.ctr, wide_a,
+                  wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
     for (void* p : ps)
       if (p) cudaFree(p);
     if (h_ctr) cudaFreeHost(h_ctr);
@@ -263,7 +265,7 @@ void init_handle(ocean_handle* h, const std::string& json) {
 // Frees the per-row arrays of a DevWork (not its counters).
 void free_work_rows(DevWork& x) {
   void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.maxb, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
-                x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf};
+                x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf, x.long_rows, x.long_acc, x.long_chunk_row};
   for (void* p : ps)
     if (p) cudaFree(p);
   DevCounters* keep = x.ctr;
@@ -292,6 +294,39 @@ void alloc_work_rows(DevWork& x, uint64_t rows) {
   OCEAN_CUDA(cudaMalloc((void**)&x.cnt, r * 4));
   OCEAN_CUDA(cudaMalloc((void**)&x.ovf, r * 4));
   x.rows = rows;
+}
+
+// The long-row list, its accumulators and the chunk -> row map for an A of
+// `rows` rows and `nnz` entries (at most nnz / kLongRowEntries rows are long,
+// and they have at most nnz / kLongChunk + that many chunks). Without them
+// (allocation failed) every row is summarised by its own lane group.
+void ensure_long_rows(DevWork& x, uint64_t nnz, uint64_t rows) {
+  const uint64_t need = std::max<uint64_t>(std::min<uint64_t>(rows, nnz / kLongRowEntries + 1), 1);
+  const uint64_t chunks = nnz / kLongChunk + need + 1;
+  if (x.long_acc && x.long_cap >= need && x.long_chunk_cap >= chunks) return;
+  void* old[] = {x.long_rows, x.long_acc, x.long_chunk_row};
+  for (void* q : old)
+    if (q) cudaFree(q);
+  x.long_rows = nullptr;
+  x.long_acc = nullptr;
+  x.long_chunk_row = nullptr;
+  x.long_cap = 0;
+  x.long_chunk_cap = 0;
+  if (chunks > 0xFFFFFFFFull) return;
+  if (cudaMalloc((void**)&x.long_rows, need * 4) != cudaSuccess ||
+      cudaMalloc((void**)&x.long_acc, need * sizeof(LongRowAcc)) != cudaSuccess ||
+      cudaMalloc((void**)&x.long_chunk_row, chunks * 4) != cudaSuccess) {
+    (void)cudaGetLastError();
+    void* got[] = {x.long_rows, x.long_acc, x.long_chunk_row};
+    for (void* q : got)
+      if (q) cudaFree(q);
+    x.long_rows = nullptr;
+    x.long_acc = nullptr;
+    x.long_chunk_row = nullptr;
+    return;
+  }
+  x.long_cap = (uint32_t)need;
+  x.long_chunk_cap = (uint32_t)chunks;
 }
 
 void ensure_rows(ocean_handle* h, uint64_t rows) {
@@ -438,6 +473,7 @@ bool run_analysis(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStrea
   h->seg_dispatch = false;  // a call dispatches by segments only after its own segmentation
   h->w.row_pol = nullptr;
   ensure_rows(h, A.rows);
+  ensure_long_rows(h->w, A.nnz, A.rows);
   OCEAN_CUDA(cudaMemsetAsync(h->w.ctr, 0, sizeof(DevCounters), s));
   SymPolicy sp;
   NumPolicy np;
@@ -763,7 +799,9 @@ int choose_workflow(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStr
       }
       if (learned) {
         // raw HLL estimates become a feature; the network then writes the estimates over them
-        h->st.launches += launch_hll_rows(A, h->w, log2p, 1.0, 0u, true, (const uint8_t*)sk, h->w.est, s);
+        // (rows of at most esc_max products take their product count and need no HLL)
+        h->st.launches += launch_hll_rows(A, h->w, log2p, 1.0, (uint32_t)c.esc_max_products, true,
+                                          (const uint8_t*)sk, h->w.est, s);
         h->st.launches += launch_mlp_estimate(model_of(h), row_inputs(h->w, B), A.rows, (uint32_t)c.esc_max_products,
                                               h->w.est, raw, &h->w.ctr->status, h->num_sms, s);
         h->st.estimator = 2;
@@ -1411,7 +1449,7 @@ void batch_pipeline(ocean_batch* b, cudaStream_t s, bool plan) {
     } else {
       launched += launch_hll_sketch_sample(A, B, w, b->log2p, 0u, b->sketch, s);
       if (b->estimator == 2) {
-        launched += launch_hll_rows(A, w, b->log2p, 1.0, 0u, true, b->sketch, w.est, s);
+        launched += launch_hll_rows(A, w, b->log2p, 1.0, sp.esc_max_products, true, b->sketch, w.est, s);
         MlpRowInputs in = row_inputs(w, B);
         in.row_problem = b->d_row_problem;
         in.problem_ctx = b->d_ctx;
@@ -1760,6 +1798,7 @@ void batch_setup(ocean_batch* b, uint64_t n, const ocean_csr_view* A, const ocea
   OCEAN_CUDA(cudaMalloc((void**)&b->d_bounds, (n + 1) * 8));
   OCEAN_CUDA(cudaHostAlloc((void**)&b->h_ctr, sizeof(DevCounters), cudaHostAllocDefault));
   alloc_work_rows(b->w, b->rows);
+  ensure_long_rows(b->w, b->nnz, b->rows);
 }
 
 // The n results as views into the plan's arena (location 2: lent by the plan).
@@ -2130,7 +2169,7 @@ int ocean_estimate(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_vie
       OCEAN_CUDA(cudaMallocAsync(&sk, std::max<uint64_t>(B->rows, 1) << log2p, s));
       launch_hll_sketch_sample(a, b, h->w, log2p, 0u, (uint8_t*)sk, s);
       if (learned) {
-        launch_hll_rows(a, h->w, log2p, 1.0, 0u, true, (const uint8_t*)sk, h->w.est, s);
+        launch_hll_rows(a, h->w, log2p, 1.0, (uint32_t)c.esc_max_products, true, (const uint8_t*)sk, h->w.est, s);
         MlpModel m = model_of(h);
         if (!with_margin) m.margin = 0.f;
         launch_mlp_estimate(m, row_inputs(h->w, b), a.rows, (uint32_t)c.esc_max_products, est, nullptr,

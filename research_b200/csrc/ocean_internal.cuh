@@ -70,7 +70,29 @@ struct DevCounters {
   unsigned int num_wide;     // numeric bitmap-class rows whose column span exceeds one 2^20-bit bitmap
   unsigned int wide_cursor;  // queue cursor of those rows' kernel (k_num_bitmap beside k_num_window)
   unsigned int usp_tile;     // fused ultra-sparse multiply: tiles handed out
+  unsigned int num_long;     // rows of A listed as long (more than kLongRowEntries entries)
+  unsigned int long_chunks;  // chunks of kLongChunk A entries of the listed rows
   unsigned int pad[1];
+};
+
+// Rows of A with more than kLongRowEntries entries are not summarised by one
+// lane group in the analysis, nor merged by one warp in the HLL row estimate:
+// one such row would keep its group busy long after every other row is done.
+// The analysis lists them and gives each a contiguous range of chunk ids (one
+// chunk = kLongChunk A entries) with a chunk -> row map; second kernels stride
+// over the chunk ids with all warps, merge the chunks' partial results into
+// the row's accumulator with atomics, and the warp that finishes a row's last
+// chunk writes the row's result.
+constexpr uint32_t kLongRowEntries = 512;
+constexpr uint32_t kLongChunk = 256;
+struct LongRowAcc {
+  unsigned long long prod;  // sum of the referenced B-row lengths
+  unsigned int lo, hi;      // smallest first column, largest last column
+  unsigned int maxb;        // longest referenced B row
+  unsigned int done;        // analysis chunks finished
+  unsigned int hdone;       // HLL chunks finished
+  unsigned int base;        // first chunk id of the row
+  unsigned int reg[64];     // HLL registers (one per word), max-merged
 };
 
 enum DevError : unsigned int {
@@ -123,16 +145,36 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-// Warp-aggregated append of `row` to bin `b` (b < 0: no append).
-__device__ __forceinline__ void bin_append(int b, uint32_t row, unsigned int* counts,
-                                           uint32_t* bins, uint64_t stride) {
+// Block-aggregated append to class lists: every thread of the block calls it
+// with R rows (b[q] < 0: no append). Offsets inside the block come from shared
+// counters (one shared atomic per warp, class and q), then one global atomic
+// per class and block reserves the block's slots: same-address global atomics
+// drop from one per warp and class to one per block and class, which is what
+// limits these kernels on inputs of many short rows. s_cnt holds `ncls`
+// zeroed counters, visible to the block before the call; ncls <= blockDim.x.
+// Block-collective (two __syncthreads).
+template <int R>
+__device__ __forceinline__ void block_bin_append(const int (&b)[R], const uint32_t (&row)[R], unsigned* s_cnt,
+                                                 int ncls, unsigned int* counts, uint32_t* bins, uint64_t stride) {
   const int lane = threadIdx.x & 31;
-  const unsigned peers = __match_any_sync(kFull, b);
-  const int leader = __ffs(peers) - 1;
-  unsigned base = 0;
-  if (lane == leader && b >= 0) base = atomicAdd(&counts[b], (unsigned)__popc(peers));
-  base = __shfl_sync(kFull, base, leader);
-  if (b >= 0) bins[(uint64_t)b * stride + base + __popc(peers & lanemask_lt())] = row;
+  unsigned off[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const unsigned peers = __match_any_sync(kFull, b[q]);
+    const int leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (lane == leader && b[q] >= 0) base = atomicAdd(&s_cnt[b[q]], (unsigned)__popc(peers));
+    off[q] = __shfl_sync(kFull, base, leader) + __popc(peers & lanemask_lt());
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < ncls) {
+    const unsigned c = s_cnt[threadIdx.x];
+    s_cnt[threadIdx.x] = c ? atomicAdd(&counts[threadIdx.x], c) : 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+    if (b[q] >= 0) bins[(uint64_t)b[q] * stride + s_cnt[b[q]] + off[q]] = row[q];
 }
 
 // Group size (lanes per A element) for a row: enough lanes to cover the mean
