@@ -672,7 +672,7 @@ def run_e2e(args, A, B, same, nnz_c, products, world, stream):
 
     pA = pin_csr(A)
     pB = pA if same else pin_csr(B)
-    g = SpGEMM({})
+    g = SpGEMM(dict(args.config))
     av, bv = pA.view(), pB.view()
     out = CsrOut()
     sptr = stream.cuda_stream
@@ -691,11 +691,13 @@ def run_e2e(args, A, B, same, nnz_c, products, world, stream):
     elapsed = max_over_ranks(e0.elapsed_time(e1), world)
     h2d = A.rowptr.nbytes + A.col.nbytes + A.val.nbytes + (0 if same else B.rowptr.nbytes + B.col.nbytes + B.val.nbytes)
     d2h = (out.rows + 1) * (out.rowptr_bits // 8) + 12 * out.nnz
+    chunks = int(g.get_stats().get("decision", {}).get("host_pipeline_chunks", 0))
     g.close()
     return {"value": round(world * 2.0 * products * steps / (elapsed / 1e3) / 1e9, 3), "unit": "GFLOP/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": steps,
-            "ms_per_step": round(elapsed / steps, 3),
-            "api": "ocean_spgemm_host (pinned host A/B in, C copied back to pinned host buffers)"}
+            "ms_per_step": round(elapsed / steps, 3), "host_pipeline_chunks": chunks,
+            "api": "ocean_spgemm_host (pinned host A/B in, C copied back to pinned host buffers; numeric phase "
+                   "in row chunks whose copies overlap the later chunks when host_pipeline_chunks > 0)"}
 
 
 # ----------------------------------------------------------------------------- further configs

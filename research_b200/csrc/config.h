@@ -201,6 +201,11 @@ struct Config {
   bool prefer_direct_hash = true;       // mid rows whose column span fits a hash table use it (direct slots)
   bool numeric_windows = false;         // exact numeric bitmap class: shared-memory value windows (k_num_window)
   bool fused_ultrasparse = false;       // ultra-sparse inputs (<= 256 products per row): one fused launch
+  // host-buffer multiplies (ocean_spgemm_host) of at least this many products
+  // run the numeric phase in row chunks of equal products and copy each
+  // finished chunk of C to the host while the next one computes (0: off)
+  int host_pipeline_chunks = 8;
+  double host_pipeline_min_products = 67108864.0;
   bool batch_autotune = false;          // batched plans: search the class policy on the batch before capturing
   std::string autotune_cache_file;      // JSON-lines cache of tuned policies (key: GPU name + batch features); "" off
   // segment-driven dispatch: rows of each spy-plot segment class take that
@@ -288,6 +293,8 @@ struct Config {
     getb("prefer_direct_hash", c.prefer_direct_hash);
     getb("numeric_windows", c.numeric_windows);
     getb("fused_ultrasparse", c.fused_ultrasparse);
+    geti("host_pipeline_chunks", c.host_pipeline_chunks);
+    getd("host_pipeline_min_products", c.host_pipeline_min_products);
     getb("batch_autotune", c.batch_autotune);
     gets("autotune_cache_file", c.autotune_cache_file);
     getb("use_segment_dispatch", c.use_segment_dispatch);

@@ -46,6 +46,14 @@ struct DevWork {
   uint32_t long_cap = 0;
   uint32_t* long_chunk_row = nullptr;  // chunk id -> index in long_rows
   uint32_t long_chunk_cap = 0;
+  // numeric class lists split into row chunks (0: one list per class): rows
+  // of chunk k are [chunk_bound[k], chunk_bound[k + 1]); class c's list of
+  // chunk k starts at num_bins[c * rows + chunk_bound[k]] with its own count
+  // and cursor (chunk_count / chunk_cursor[c * chunks + k])
+  int chunks = 0;
+  uint32_t* chunk_bound = nullptr;
+  unsigned* chunk_count = nullptr;
+  unsigned* chunk_cursor = nullptr;
   // segment-driven dispatch: per-row policy slot (0: the call's policy,
   // 1 + SegClass: that segment class's policy); null: slot 0 for every row
   const uint8_t* row_pol = nullptr;
@@ -157,10 +165,19 @@ template <typename RP>
 int launch_overflow(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, bool numeric, uint32_t* c_col,
                     double* c_val, int num_sms, cudaStream_t s);
 
+// chunk >= 0 (w.chunks > 0): only the rows of that row chunk, from its
+// per-chunk class lists (row_base = its first row); counts are then the
+// chunk's class sizes.
 template <typename RP>
 int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const OutSpec& out, uint32_t* c_col,
                     double* c_val, int num_sms, cudaStream_t s, cudaEvent_t* bin_events,
-                    const unsigned* counts = nullptr);
+                    const unsigned* counts = nullptr, int chunk = -1, uint32_t row_base = 0);
+
+// Row chunks of equal products for a chunked numeric phase: with prefix[] the
+// exclusive scan of the per-row products (rows + 1 values), w.chunk_bound[k] =
+// the first row whose prefix reaches k/chunks of the total (k = 0 .. chunks).
+constexpr int kMaxChunks = 16;
+void launch_chunk_bounds(const DevWork& w, const uint64_t* prefix, int chunks, cudaStream_t s);
 
 void launch_murmur3(const uint32_t* keys, uint32_t* out, uint64_t n, uint32_t seed, cudaStream_t s);
 

@@ -298,7 +298,8 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
   {
     const int bq[1] = {b};
     const uint32_t rq[1] = {(uint32_t)row};
-    block_bin_append<1>(bq, rq, s_cnt, SB_COUNT, ctr->sym_count, sym_bins, A.rows);
+    const int sq[1] = {0};
+    block_bin_append<1>(bq, sq, rq, s_cnt, SB_COUNT, 1, nullptr, ctr->sym_count, nullptr, sym_bins, A.rows);
   }
   if (threadIdx.x < SB_COUNT) {
     if (s_anz[threadIdx.x]) atomicAdd(&ctr->sym_anz[threadIdx.x], s_anz[threadIdx.x]);
@@ -2062,12 +2063,17 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
                                                      const uint64_t* __restrict__ bm_off,
                                                      uint32_t* __restrict__ num_bins,
                                                      DevCounters* __restrict__ ctr, NumPolicySet pols,
-                                                     const uint8_t* __restrict__ row_pol, int bin_rows) {
+                                                     const uint8_t* __restrict__ row_pol, int bin_rows, int chunks,
+                                                     const uint32_t* __restrict__ chunk_bound,
+                                                     unsigned* __restrict__ chunk_count) {
   __shared__ unsigned long long scr[33];
   __shared__ unsigned long long s_cls[3][NB_COUNT];
-  __shared__ unsigned s_cnt[NB_COUNT];
+  __shared__ unsigned s_cnt[NB_COUNT * kMaxChunks];
+  __shared__ uint32_t s_bound[kMaxChunks + 1];
+  const int nseg = chunks > 1 ? chunks : 1;
   if (threadIdx.x < 3 * NB_COUNT) (&s_cls[0][0])[threadIdx.x] = 0ull;
-  if (threadIdx.x < NB_COUNT) s_cnt[threadIdx.x] = 0u;
+  if (threadIdx.x < NB_COUNT * kMaxChunks) s_cnt[threadIdx.x] = 0u;
+  if (nseg > 1 && (int)threadIdx.x <= nseg) s_bound[threadIdx.x] = chunk_bound[threadIdx.x];
   const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * 4;
   uint32_t v[4];
   unsigned long long s = 0;
@@ -2078,7 +2084,7 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
   }
   unsigned long long total;
   unsigned long long run = block_excl_scan<1024, unsigned long long>(s, scr, &total) + tile_offs[blockIdx.x];
-  int bq[4];
+  int bq[4], sq[4];
   uint32_t rq[4], aq[4], pq[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -2100,9 +2106,16 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
     }
     bq[q] = b;
     rq[q] = (uint32_t)i;
+    // row chunk of the row: the last chunk whose first row is <= i (the
+    // bounds are visible after the block scan's barriers)
+    int g = 0;
+    if (nseg > 1 && b >= 0)
+      while (g + 1 < nseg && s_bound[g + 1] <= i) ++g;
+    sq[q] = g;
   }
   if (!bin_rows) return;
-  block_bin_append<4>(bq, rq, s_cnt, NB_COUNT, ctr->num_count, num_bins, n);
+  block_bin_append<4>(bq, sq, rq, s_cnt, NB_COUNT, nseg, s_bound, nseg > 1 ? chunk_count : ctr->num_count,
+                      ctr->num_count, num_bins, n);
   // per-class sums (nnz, A entries, products) of the classes present in the
   // warp: warp sums, then one shared atomic per warp and class
   const int lane = threadIdx.x & 31;
@@ -2622,14 +2635,42 @@ int launch_scan(const DevWork& w, const uint32_t* in, uint64_t* out64, uint32_t*
   const uint8_t* row_pol = seg ? w.row_pol : nullptr;
   k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(in, w.rows, w.tile_sums);
   k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, total, out64, out32, w.rows);
+  const int chunks = bin_rows ? w.chunks : 0;
   k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(in, w.rows, w.tile_sums, out64, out32, w.prod, w.lo, w.hi, w.anz,
-                                             w.bm_off, w.num_bins, w.ctr, pols, row_pol, bin_rows ? 1 : 0);
+                                             w.bm_off, w.num_bins, w.ctr, pols, row_pol, bin_rows ? 1 : 0, chunks,
+                                             w.chunk_bound, w.chunk_count);
   return 3;
+}
+
+// bound[k] = first row r with prefix[r] >= ceil(k * total / chunks), by binary
+// search; bound[0] = 0, bound[chunks] = rows. One thread per bound.
+__global__ void k_chunk_bounds(const uint64_t* __restrict__ prefix, uint64_t rows, int chunks,
+                               uint32_t* __restrict__ bound) {
+  const int k = threadIdx.x;
+  if (k > chunks) return;
+  const uint64_t total = prefix[rows];
+  if (k == 0 || k == chunks) {
+    bound[k] = k == 0 ? 0u : (uint32_t)rows;
+    return;
+  }
+  const uint64_t target = (total * (uint64_t)k + chunks - 1) / chunks;
+  uint64_t lo = 0, hi = rows;  // first r in [0, rows] with prefix[r] >= target
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (prefix[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  bound[k] = (uint32_t)lo;
+}
+
+void launch_chunk_bounds(const DevWork& w, const uint64_t* prefix, int chunks, cudaStream_t s) {
+  k_chunk_bounds<<<1, 32, 0, s>>>(prefix, w.rows, chunks, w.chunk_bound);
 }
 
 template <typename RP>
 int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const OutSpec& o, uint32_t* c_col,
-                   double* c_val, int num_sms, cudaStream_t s, cudaEvent_t* ev, const unsigned* counts) {
+                   double* c_val, int num_sms, cudaStream_t s, cudaEvent_t* ev, const unsigned* counts, int chunk,
+                   uint32_t row_base) {
   if (A.rows == 0) return 0;
   int launched = 0;
   auto mark = [&](int i) {
@@ -2638,7 +2679,12 @@ int launch_numeric(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const O
   auto grid = [&](int kind, int cls, unsigned per_block) {
     return class_grid(num_sms, g_occ[kind], counts, cls, per_block);
   };
+  const bool chunked = chunk >= 0 && w.chunks > 1;
   auto queue = [&](int c) {
+    if (chunked) {
+      const int slot = c * w.chunks + chunk;
+      return RowQueue{w.num_bins + (uint64_t)c * A.rows + row_base, w.chunk_count + slot, w.chunk_cursor + slot};
+    }
     return RowQueue{w.num_bins + (uint64_t)c * A.rows, w.ctr->num_count + c, w.ctr->num_cursor + c};
   };
   unsigned gsz;
@@ -2798,8 +2844,10 @@ template int launch_symbolic<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>
 template int launch_symbolic<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, int,
                                         cudaStream_t, cudaEvent_t*, const unsigned*);
 template int launch_numeric<uint32_t>(const Csr<uint32_t>&, const Csr<uint32_t>&, const DevWork&, const OutSpec&,
-                                      uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*);
+                                      uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*, int,
+                                      uint32_t);
 template int launch_numeric<uint64_t>(const Csr<uint64_t>&, const Csr<uint64_t>&, const DevWork&, const OutSpec&,
-                                      uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*);
+                                      uint32_t*, double*, int, cudaStream_t, cudaEvent_t*, const unsigned*, int,
+                                      uint32_t);
 
 }  // namespace ocean

@@ -93,6 +93,7 @@ struct Stats {
   uint64_t cache_words = 0, cache_used = 0;
   bool cache_dropped = false;
   int bm_kernel = 0;  // numeric bitmap class: 0 no rows, 1 k_num_bitmap (rank + FP64 red), 2 k_num_window
+  int host_chunks = 0;  // host-buffer multiply: row chunks whose copies overlapped the numeric phase (0: none)
   bool fused = false;  // ultra-sparse workflow in one fused launch
   int launches = 0;  // kernels launched by the last call
   uint64_t total_est = 0, overflow_rows = 0;
@@ -208,6 +209,15 @@ struct ocean_handle {
   uint64_t win_cursor_cap = 0;
   unsigned long long* win_scratch = nullptr;
   uint64_t win_scratch_cap = 0;
+  // host-buffer multiply (ocean_spgemm_host) under way: the precise workflow
+  // may run its numeric phase in row chunks and copy each finished chunk of C
+  // to the pinned host buffers on copy_stream (sink_filled: it did)
+  bool sink_active = false;
+  bool sink_filled = false;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t chunk_ev[kMaxChunks + 1] = {};
+  uint32_t* chunk_dev = nullptr;  // bounds (kMaxChunks + 1), counts and cursors (NB_COUNT x kMaxChunks each)
+  uint32_t* chunk_host = nullptr; // pinned: bounds and counts read back
 
   void free_all() {
     DevWork& x = w;
@@ -225,6 +235,11 @@ struct ocean_handle {
     if (usp_tiles_buf) cudaFree(usp_tiles_buf);
     if (win_cursor) cudaFree(win_cursor);
     if (win_scratch) cudaFree(win_scratch);
+    if (chunk_dev) cudaFree(chunk_dev);
+    if (chunk_host) cudaFreeHost(chunk_host);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    for (auto& e : chunk_ev)
+      if (e) cudaEventDestroy(e);
     if (mlp_dev) cudaFree(mlp_dev);
     if (raw_est) cudaFree(raw_est);
     if (row_pol) cudaFree(row_pol);
@@ -867,6 +882,54 @@ void alloc_c(ocean_handle* h, CResult* owner, uint64_t rows, uint64_t nnz, int b
   OCEAN_CUDA(e);
 }
 
+// The chunked numeric phase of a host-buffer multiply (h->w.chunks > 0, the
+// chunk bounds and class sizes read back into h->chunk_host): C's row
+// pointers go to the pinned host buffer first; then for every row chunk its
+// numeric class kernels run on s, and an event lets copy_stream copy the
+// chunk's column ids and values (contiguous in C) to the host while the
+// following chunks compute. s waits for the copies at the end, so the caller's
+// stream order covers them. Returns the kernels launched.
+template <typename RP>
+int pipeline_numeric(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, const OutSpec& exact, CResult* owner,
+                     uint64_t nnz, int bits, cudaStream_t s) {
+  const int k = h->w.chunks;
+  const uint32_t* bound = h->chunk_host;
+  const uint32_t* counts = h->chunk_host + (kMaxChunks + 1);
+  const uint64_t rpb = (A.rows + 1) * (uint64_t)(bits / 8);
+  grow_host(h->out_rp, h->out_rp_cap, rpb);
+  grow_host(h->out_col, h->out_col_cap, nnz);
+  grow_host(h->out_val, h->out_val_cap, nnz);
+  OCEAN_CUDA(cudaMemcpyAsync(h->out_rp, bits == 64 ? (void*)h->w.rowptr64 : (void*)h->w.rowptr32, rpb,
+                             cudaMemcpyDeviceToHost, s));
+  OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
+  auto offset = [&](uint32_t r) -> uint64_t {
+    return bits == 64 ? ((const uint64_t*)h->out_rp)[r] : (uint64_t)((const uint32_t*)h->out_rp)[r];
+  };
+  int launched = 0;
+  for (int c = 0; c < k; ++c) {
+    const uint32_t r0 = bound[c], r1 = bound[c + 1];
+    if (r1 <= r0) continue;
+    unsigned cc[NB_COUNT];
+    for (int i = 0; i < NB_COUNT; ++i) cc[i] = counts[i * k + c];
+    launched += launch_numeric(A, B, h->w, exact, owner->col, owner->val, h->num_sms, s, nullptr, cc, c, r0);
+    OCEAN_CUDA(cudaEventRecord(h->chunk_ev[c], s));
+    OCEAN_CUDA(cudaStreamWaitEvent(h->copy_stream, h->chunk_ev[c], 0));
+    const uint64_t o0 = offset(r0), o1 = offset(r1);
+    if (o1 > o0) {
+      OCEAN_CUDA(cudaMemcpyAsync(h->out_col + o0, owner->col + o0, (o1 - o0) * 4, cudaMemcpyDeviceToHost,
+                                 h->copy_stream));
+      OCEAN_CUDA(cudaMemcpyAsync(h->out_val + o0, owner->val + o0, (o1 - o0) * 8, cudaMemcpyDeviceToHost,
+                                 h->copy_stream));
+    }
+  }
+  OCEAN_CUDA(cudaEventRecord(h->chunk_ev[kMaxChunks], h->copy_stream));
+  OCEAN_CUDA(cudaStreamWaitEvent(s, h->chunk_ev[kMaxChunks], 0));
+  h->st.host_chunks = k;
+  h->w.chunks = 0;
+  h->sink_filled = true;
+  return launched;
+}
+
 template <typename RP>
 void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view* Bv, const RP* arp,
                 const RP* brp, ocean_csr* C, cudaStream_t s) {
@@ -964,11 +1027,42 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
           OCEAN_CUDA(cudaMemsetAsync(h->w.ctr->num_count, 0, sizeof(unsigned) * NB_COUNT * 2, s));
         }
       }
+      // host-buffer multiplies of many products: the numeric phase runs in
+      // row chunks of equal products (the scan splits the class lists by
+      // chunk) so that each chunk's copy to the host overlaps the next ones
+      h->w.chunks = 0;
+      if (h->sink_active && wf == WF_PRECISE && readback && !st.fused && !cf.numeric_windows && !track &&
+          cf.host_pipeline_chunks > 1 && (double)h->h_ctr->total_products >= cf.host_pipeline_min_products) {
+        const int k = std::min(cf.host_pipeline_chunks, kMaxChunks);
+        const size_t words = (kMaxChunks + 1) + 2 * NB_COUNT * kMaxChunks;
+        if (!h->chunk_dev) {
+          OCEAN_CUDA(cudaMalloc((void**)&h->chunk_dev, words * 4));
+          OCEAN_CUDA(cudaHostAlloc((void**)&h->chunk_host, words * 4, cudaHostAllocDefault));
+        }
+        if (!h->copy_stream) {
+          OCEAN_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+          for (auto& e : h->chunk_ev) OCEAN_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        h->w.chunks = k;
+        h->w.chunk_bound = h->chunk_dev;
+        h->w.chunk_count = h->chunk_dev + (kMaxChunks + 1);
+        h->w.chunk_cursor = h->w.chunk_count + NB_COUNT * kMaxChunks;
+        OCEAN_CUDA(cudaMemsetAsync(h->w.chunk_count, 0, 2 * NB_COUNT * kMaxChunks * 4, s));
+        // exclusive scan of the products (into est_off, unused by this workflow), then the bounds
+        st.launches += launch_scan(h->w, h->w.prod, h->w.est_off, nullptr, &h->w.ctr->total_est, false, np, s);
+        launch_chunk_bounds(h->w, h->w.est_off, k, s);
+        st.launches += 1;
+      }
       if (st.fused) {
       } else if (wf == WF_PRECISE) {
         run_symbolic(h, A, B, s, readback, true, true);
         mark("symbolic");
         nnz = h->h_ctr->total_nnz;
+        if (h->w.chunks) {
+          OCEAN_CUDA(cudaMemcpyAsync(h->chunk_host, h->chunk_dev, ((kMaxChunks + 1) + NB_COUNT * kMaxChunks) * 4,
+                                     cudaMemcpyDeviceToHost, s));
+          OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
+        }
       } else {
         OCEAN_CUDA(cudaMallocAsync(&t_col, std::max<uint64_t>(st.total_est, 1) * 4, s));
         OCEAN_CUDA(cudaMallocAsync(&t_val, std::max<uint64_t>(st.total_est, 1) * 8, s));
@@ -1018,8 +1112,12 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         for (int i = 0; i < NB_COUNT; ++i) num_counts[i] = h->h_ctr->num_count[i];
         prepare_windows(h, A.nnz, num_counts[NB_BITMAP]);
         const OutSpec exact{h->w.rowptr64, h->w.row_nnz, nullptr, nullptr, nullptr};
-        st.launches += launch_numeric(A, B, h->w, exact, owner->col, owner->val, h->num_sms, s,
-                                      track ? h->ev + EV_NUM0 : nullptr, num_counts);
+        if (h->w.chunks) {
+          st.launches += pipeline_numeric(h, A, B, exact, owner, nnz, bits, s);
+        } else {
+          st.launches += launch_numeric(A, B, h->w, exact, owner->col, owner->val, h->num_sms, s,
+                                        track ? h->ev + EV_NUM0 : nullptr, num_counts);
+        }
         if (track) h->ev_mask |= ((1ull << (NB_COUNT + 1)) - 1) << EV_NUM0;
       } else {
         launch_copy_rows(h->w, (const uint32_t*)t_col, (const double*)t_val, owner->col, owner->val, s);
@@ -1050,6 +1148,8 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
       mark("synced");
     }
   } catch (...) {
+    h->w.chunks = 0;
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);  // no copy may still read C
     release_cache(h, s);
     if (t_col) cudaFreeAsync(t_col, s);
     if (t_val) cudaFreeAsync(t_val, s);
@@ -1153,7 +1253,7 @@ std::string stats_json(ocean_handle* h) {
     << ", \"bitmap_cache_dropped\": " << (st.cache_dropped ? "true" : "false")
     << ", \"fused_ultrasparse\": " << (st.fused ? "true" : "false")
     << ", \"numeric_bitmap_kernel\": \"" << (st.bm_kernel == 2 ? "window" : st.bm_kernel == 1 ? "rank" : "none")
-    << "\", \"kernel_launches\": " << st.launches << "}, ";
+    << "\", \"host_pipeline_chunks\": " << st.host_chunks << ", \"kernel_launches\": " << st.launches << "}, ";
   if (st.sampled)
     o << "\"sampling\": {\"compaction_1\": " << st.compaction1 << ", \"compaction_2\": " << st.compaction2
       << "}, ";
@@ -1910,17 +2010,29 @@ int ocean_spgemm_host(ocean_handle* h, const ocean_csr_view* A, const ocean_csr_
     if (same) dv[1] = dv[0];
     ocean_csr dc;
     const auto t_in = std::chrono::steady_clock::now();
-    dispatch_spgemm(h, &dv[0], &dv[1], &dc, s);
+    // large precise multiplies copy C to the pinned host buffers chunk by
+    // chunk from inside the numeric phase (pipeline_numeric)
+    h->sink_active = true;
+    h->sink_filled = false;
+    try {
+      dispatch_spgemm(h, &dv[0], &dv[1], &dc, s);
+    } catch (...) {
+      h->sink_active = false;
+      throw;
+    }
+    h->sink_active = false;
     const uint64_t rpb = (dc.rows + 1) * (uint64_t)(dc.rowptr_bits / 8);
     CResult* dev_owner = (CResult*)dc._owner;
     try {
-      grow_host(h->out_rp, h->out_rp_cap, rpb);
-      grow_host(h->out_col, h->out_col_cap, dc.nnz);
-      grow_host(h->out_val, h->out_val_cap, dc.nnz);
-      OCEAN_CUDA(cudaMemcpyAsync(h->out_rp, dc.rowptr, rpb, cudaMemcpyDeviceToHost, s));
-      if (dc.nnz) {
-        OCEAN_CUDA(cudaMemcpyAsync(h->out_col, dc.col, dc.nnz * 4, cudaMemcpyDeviceToHost, s));
-        OCEAN_CUDA(cudaMemcpyAsync(h->out_val, dc.val, dc.nnz * 8, cudaMemcpyDeviceToHost, s));
+      if (!h->sink_filled) {
+        grow_host(h->out_rp, h->out_rp_cap, rpb);
+        grow_host(h->out_col, h->out_col_cap, dc.nnz);
+        grow_host(h->out_val, h->out_val_cap, dc.nnz);
+        OCEAN_CUDA(cudaMemcpyAsync(h->out_rp, dc.rowptr, rpb, cudaMemcpyDeviceToHost, s));
+        if (dc.nnz) {
+          OCEAN_CUDA(cudaMemcpyAsync(h->out_col, dc.col, dc.nnz * 4, cudaMemcpyDeviceToHost, s));
+          OCEAN_CUDA(cudaMemcpyAsync(h->out_val, dc.val, dc.nnz * 8, cudaMemcpyDeviceToHost, s));
+        }
       }
     } catch (...) {
       cudaFreeAsync(dev_owner->rowptr, s);

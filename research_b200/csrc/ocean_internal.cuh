@@ -146,35 +146,46 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 }
 
 // Block-aggregated append to class lists: every thread of the block calls it
-// with R rows (b[q] < 0: no append). Offsets inside the block come from shared
-// counters (one shared atomic per warp, class and q), then one global atomic
-// per class and block reserves the block's slots: same-address global atomics
-// drop from one per warp and class to one per block and class, which is what
-// limits these kernels on inputs of many short rows. s_cnt holds `ncls`
-// zeroed counters, visible to the block before the call; ncls <= blockDim.x.
+// with R rows (b[q] < 0: no append), each in list segment seg[q] (one segment
+// per row chunk; 0 when the lists are not split). Offsets inside the block
+// come from shared counters (one shared atomic per warp, class, segment and
+// q), then one global atomic per class, segment and block reserves the
+// block's slots: same-address global atomics drop from one per warp and class
+// to one per block and class, which is what limits these kernels on inputs of
+// many short rows. Segment g of class c starts at bins[c * stride +
+// seg_base[g]] and counts into counts[c * nseg + g]; with nseg > 1 the class
+// totals also go to totals[c]. s_cnt holds ncls * nseg zeroed counters,
+// visible to the block before the call; ncls * nseg <= blockDim.x.
 // Block-collective (two __syncthreads).
 template <int R>
-__device__ __forceinline__ void block_bin_append(const int (&b)[R], const uint32_t (&row)[R], unsigned* s_cnt,
-                                                 int ncls, unsigned int* counts, uint32_t* bins, uint64_t stride) {
+__device__ __forceinline__ void block_bin_append(const int (&b)[R], const int (&seg)[R], const uint32_t (&row)[R],
+                                                 unsigned* s_cnt, int ncls, int nseg, const uint32_t* seg_base,
+                                                 unsigned int* counts, unsigned int* totals, uint32_t* bins,
+                                                 uint64_t stride) {
   const int lane = threadIdx.x & 31;
   unsigned off[R];
 #pragma unroll
   for (int q = 0; q < R; ++q) {
-    const unsigned peers = __match_any_sync(kFull, b[q]);
+    const int slot = b[q] >= 0 ? b[q] * nseg + seg[q] : -1;
+    const unsigned peers = __match_any_sync(kFull, slot);
     const int leader = __ffs(peers) - 1;
     unsigned base = 0;
-    if (lane == leader && b[q] >= 0) base = atomicAdd(&s_cnt[b[q]], (unsigned)__popc(peers));
+    if (lane == leader && slot >= 0) base = atomicAdd(&s_cnt[slot], (unsigned)__popc(peers));
     off[q] = __shfl_sync(kFull, base, leader) + __popc(peers & lanemask_lt());
   }
   __syncthreads();
-  if ((int)threadIdx.x < ncls) {
+  const int nslot = ncls * nseg;
+  if ((int)threadIdx.x < nslot) {
     const unsigned c = s_cnt[threadIdx.x];
+    if (c && nseg > 1) atomicAdd(&totals[threadIdx.x / nseg], c);
     s_cnt[threadIdx.x] = c ? atomicAdd(&counts[threadIdx.x], c) : 0u;
   }
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < R; ++q)
-    if (b[q] >= 0) bins[(uint64_t)b[q] * stride + s_cnt[b[q]] + off[q]] = row[q];
+    if (b[q] >= 0)
+      bins[(uint64_t)b[q] * stride + (nseg > 1 ? seg_base[seg[q]] : 0u) + s_cnt[b[q] * nseg + seg[q]] + off[q]] =
+          row[q];
 }
 
 // Group size (lanes per A element) for a row: enough lanes to cover the mean
