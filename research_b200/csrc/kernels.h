@@ -46,6 +46,10 @@ struct DevWork {
   uint32_t long_cap = 0;
   uint32_t* long_chunk_row = nullptr;  // chunk id -> index in long_rows
   uint32_t long_chunk_cap = 0;
+  // per row of B: first column, last column, length (low, high word); built
+  // at the start of each analysis (null: the analysis reads B itself)
+  uint4* btab = nullptr;
+  uint64_t btab_cap = 0;
   // numeric class lists split into row chunks (0: one list per class): rows
   // of chunk k are [chunk_bound[k], chunk_bound[k + 1]); class c's list of
   // chunk k starts at num_bins[c * rows + chunk_bound[k]] with its own count

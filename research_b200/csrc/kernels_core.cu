@@ -127,12 +127,46 @@ __device__ __forceinline__ uint32_t spread_index(uint32_t idx, uint32_t count, u
 }
 
 // ---------------------------------------------------------------- analysis
+// Row table of B for the analysis: first column, last column and length of
+// every row in one 16-byte entry, so an A entry costs one load of a table
+// that stays in L2 instead of its B row's pointers and two column loads.
+template <typename RP>
+__global__ void __launch_bounds__(256) k_brow_table(Csr<RP> B, uint4* __restrict__ tab) {
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < B.rows;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t b0 = B.row_begin(r), b1 = B.row_end(r);
+    const uint64_t len = b1 - b0;
+    tab[r] = make_uint4(len ? B.col[b0] : kEmpty, len ? B.col[b1 - 1] : 0u, (uint32_t)len, (uint32_t)(len >> 32));
+  }
+}
+
 // Products, smallest first column, largest last column and longest B row
 // over A entries k0, k0 + G, k0 + 2G, ... below k1, accumulated into p, mn,
-// mx, lb. Four entries per pass have their dependent loads in flight together.
+// mx, lb. Four entries per pass have their dependent loads in flight together;
+// with the row table of B (btab) each entry is one table load.
 template <int G, typename RP>
-__device__ __forceinline__ void span_part(const Csr<RP>& A, const Csr<RP>& B, uint64_t k0, uint64_t k1,
-                                          unsigned long long& p, uint32_t& mn, uint32_t& mx, uint32_t& lb) {
+__device__ __forceinline__ void span_part(const Csr<RP>& A, const Csr<RP>& B, const uint4* __restrict__ btab,
+                                          uint64_t k0, uint64_t k1, unsigned long long& p, uint32_t& mn,
+                                          uint32_t& mx, uint32_t& lb) {
+  if (btab) {
+    for (; k0 < k1; k0 += 4 * G) {
+      uint4 t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        t[u] = k0 + (uint64_t)u * G < k1 ? btab[A.col[k0 + (uint64_t)u * G]] : make_uint4(kEmpty, 0u, 0u, 0u);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint64_t len = (uint64_t)t[u].z | ((uint64_t)t[u].w << 32);
+        if (len) {
+          p += len;
+          mn = min(mn, t[u].x);
+          mx = max(mx, t[u].y);
+          lb = max(lb, (uint32_t)min(len, (uint64_t)0xFFFFFFFFu));
+        }
+      }
+    }
+    return;
+  }
   for (; k0 < k1; k0 += 4 * G) {
     uint32_t j[4];
 #pragma unroll
@@ -195,7 +229,8 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
                                                   const uint8_t* __restrict__ row_pol,
                                                   uint32_t* __restrict__ long_rows,
                                                   LongRowAcc* __restrict__ long_acc, uint32_t long_cap,
-                                                  uint32_t* __restrict__ long_chunk_row, uint32_t chunk_cap) {
+                                                  uint32_t* __restrict__ long_chunk_row, uint32_t chunk_cap,
+                                                  const uint4* __restrict__ btab) {
   __shared__ unsigned long long s_anz[SB_COUNT], s_prod[SB_COUNT], s_words, s_tot;
   __shared__ unsigned s_maxp, s_maxa, s_cnt[SB_COUNT];
   if (threadIdx.x < SB_COUNT) {
@@ -222,7 +257,7 @@ __global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t
   const bool is_long = long_acc != nullptr && a1 - a0 > kLongRowEntries;  // uniform in the group
   unsigned long long p = 0;
   uint32_t mn = kEmpty, mx = 0, lb = 0;
-  if (!is_long) span_part<G>(A, B, a0 + sl, a1, p, mn, mx, lb);
+  if (!is_long) span_part<G>(A, B, btab, a0 + sl, a1, p, mn, mx, lb);
 #pragma unroll
   for (int o = G / 2; o > 0; o >>= 1) {
     p += __shfl_xor_sync(kFull, p, o);
@@ -328,7 +363,7 @@ __global__ void __launch_bounds__(256) k_analysis_long(Csr<RP> A, Csr<RP> B, uin
                                                        const uint32_t* __restrict__ long_rows,
                                                        LongRowAcc* __restrict__ long_acc, uint32_t long_cap,
                                                        const uint32_t* __restrict__ long_chunk_row,
-                                                       uint32_t chunk_cap) {
+                                                       uint32_t chunk_cap, const uint4* __restrict__ btab) {
   const uint32_t total = min(ctr->long_chunks, chunk_cap);
   const uint32_t nl = min(ctr->num_long, long_cap);
   const int lane = threadIdx.x & 31;
@@ -344,7 +379,7 @@ __global__ void __launch_bounds__(256) k_analysis_long(Csr<RP> A, Csr<RP> B, uin
     const uint64_t c0 = a0 + (uint64_t)(c - L.base) * kLongChunk;
     unsigned long long p = 0;
     uint32_t mn = kEmpty, mx = 0, lb = 0;
-    span_part<32>(A, B, c0 + lane, min(a1, c0 + kLongChunk), p, mn, mx, lb);
+    span_part<32>(A, B, btab, c0 + lane, min(a1, c0 + kLongChunk), p, mn, mx, lb);
     p = warp_sum_u64(p);
     mn = __reduce_min_sync(kFull, mn);
     mx = __reduce_max_sync(kFull, mx);
@@ -2553,22 +2588,31 @@ int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const 
   const int g = avg <= 16.0 ? 4 : avg <= 32.0 ? 8 : avg <= 64.0 ? 16 : 32;
   const uint64_t per_block = 256 / g;
   const unsigned blocks = (unsigned)((A.rows + per_block - 1) / per_block);
+  int launched = 0;
+  // the row table of B pays from about a million entries of B (config 1,
+  // 0.33 M entries: its extra launch costs more than it saves)
+  const uint4* btab = (w.btab && B.nnz >= (1ull << 20)) ? w.btab : nullptr;
+  if (btab) {
+    k_brow_table<RP><<<(unsigned)std::min<uint64_t>((B.rows + 255) / 256, 148ull * 16), 256, 0, s>>>(B, w.btab);
+    ++launched;
+  }
 #define OCEAN_ANALYSIS(G)                                                                                          \
   k_analysis<RP, G><<<blocks, 256, 0, s>>>(A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off, w.sym_bins, \
                                            w.ctr, pols, row_pol, w.long_rows, w.long_acc, w.long_cap, w.long_chunk_row, \
-                                           w.long_chunk_cap)
+                                           w.long_chunk_cap, btab)
   if (g == 32) OCEAN_ANALYSIS(32);
   else if (g == 16) OCEAN_ANALYSIS(16);
   else if (g == 8) OCEAN_ANALYSIS(8);
   else OCEAN_ANALYSIS(4);
 #undef OCEAN_ANALYSIS
+  ++launched;
   if (w.long_acc) {
     k_analysis_long<RP><<<4 * 148, 256, 0, s>>>(A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off,
                                                 w.sym_bins, w.ctr, pols, row_pol, w.long_rows, w.long_acc, w.long_cap,
-                                                w.long_chunk_row, w.long_chunk_cap);
-    return 2;
+                                                w.long_chunk_row, w.long_chunk_cap, btab);
+    ++launched;
   }
-  return 1;
+  return launched;
 }
 
 // Grid of a persistent class kernel: resident blocks on all SMs, capped by

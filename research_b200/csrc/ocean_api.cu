@@ -223,7 +223,7 @@ struct ocean_handle {
     DevWork& x = w;
     void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.maxb, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
                   x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf, x.long_rows, x.long_acc, x.long_chunk_row,
-                  x.ctr, wide_a,
+                  x.btab, x.ctr, wide_a,
                   wide_b, in_rp[0], in_rp[1], in_col[0], in_col[1], in_val[0], in_val[1]};
     for (void* p : ps)
       if (p) cudaFree(p);
@@ -280,7 +280,8 @@ void init_handle(ocean_handle* h, const std::string& json) {
 // Frees the per-row arrays of a DevWork (not its counters).
 void free_work_rows(DevWork& x) {
   void* ps[] = {x.prod, x.lo, x.hi, x.anz, x.maxb, x.row_nnz, x.sym_bins, x.num_bins, x.tile_sums, x.rowptr64,
-                x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf, x.long_rows, x.long_acc, x.long_chunk_row};
+                x.rowptr32, x.bm_off, x.est, x.est_off, x.cnt, x.ovf, x.long_rows, x.long_acc, x.long_chunk_row,
+                x.btab};
   for (void* p : ps)
     if (p) cudaFree(p);
   DevCounters* keep = x.ctr;
@@ -342,6 +343,22 @@ void ensure_long_rows(DevWork& x, uint64_t nnz, uint64_t rows) {
   }
   x.long_cap = (uint32_t)need;
   x.long_chunk_cap = (uint32_t)chunks;
+}
+
+// The row table of B (16 B per row of B, grow-only). Without it (allocation
+// failed) the analysis reads B's rows itself.
+void ensure_btab(DevWork& x, uint64_t b_rows) {
+  const uint64_t need = std::max<uint64_t>(b_rows, 1);
+  if (x.btab && x.btab_cap >= need) return;
+  if (x.btab) cudaFree(x.btab);
+  x.btab = nullptr;
+  x.btab_cap = 0;
+  if (cudaMalloc((void**)&x.btab, need * sizeof(uint4)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    x.btab = nullptr;
+    return;
+  }
+  x.btab_cap = need;
 }
 
 void ensure_rows(ocean_handle* h, uint64_t rows) {
@@ -489,6 +506,7 @@ bool run_analysis(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStrea
   h->w.row_pol = nullptr;
   ensure_rows(h, A.rows);
   ensure_long_rows(h->w, A.nnz, A.rows);
+  ensure_btab(h->w, B.rows);
   OCEAN_CUDA(cudaMemsetAsync(h->w.ctr, 0, sizeof(DevCounters), s));
   SymPolicy sp;
   NumPolicy np;
@@ -1899,6 +1917,7 @@ void batch_setup(ocean_batch* b, uint64_t n, const ocean_csr_view* A, const ocea
   OCEAN_CUDA(cudaHostAlloc((void**)&b->h_ctr, sizeof(DevCounters), cudaHostAllocDefault));
   alloc_work_rows(b->w, b->rows);
   ensure_long_rows(b->w, b->nnz, b->rows);
+  ensure_btab(b->w, b->brows);
 }
 
 // The n results as views into the plan's arena (location 2: lent by the plan).
