@@ -404,10 +404,10 @@ def run_reference(args, world, rank):
 
 def reference_gpu_build(names=("laplacian256", "rect")) -> dict:
     """The reference's own CUDA build (oracle/_ref/spgemm_ref, compiled from
-    its sources with NUM_SM = 148 by `make -C oracle refbin`) on configs 1 and
-    3, through its own driver with 10 warm-up and 10 timed iterations; its
+    its sources with NUM_SM = 148 by `make -C oracle refbin`) on the Laplacian
+    256^2 and the rectangular A*A^T, through its own driver with 10 warm-up and 10 timed iterations; its
     stats JSON gives its mean time per multiply. Skipped where the build or a
-    GPU is missing. (Config 2 is not run: nnz(C) exceeds the reference's
+    GPU is missing. (The R-MAT 2^20 multiply is not run: nnz(C) exceeds the reference's
     32-bit row offsets, and a wrapped offset would write out of bounds.)"""
     import shutil
     import tempfile
@@ -700,13 +700,13 @@ def run_e2e(args, A, B, same, nnz_c, products, world, stream):
                    "in row chunks whose copies overlap the later chunks when host_pipeline_chunks > 0)"}
 
 
-# ----------------------------------------------------------------------------- further configs
+# ----------------------------------------------------------------------------- further workloads
 # The default run also measures the metric's other forms on one GPU, each with
 # its own fixed, small step counts so the whole run stays within minutes:
-# configs 1 and 3 (Laplacian 256^2 and the rectangular A*A^T) as plain calls,
-# as a one-problem captured plan and end to end; config 4 (learned row sizing
-# of the held-out R-MAT 2^21 against HLL and exact counts); config 5 (512
-# products: learned + batched against 512 plain calls, with the HLL- and
+# the Laplacian 256^2 and the rectangular A*A^T as plain calls, as a
+# one-problem captured plan and end to end; learned row sizing of the
+# held-out R-MAT 2^21 against HLL and exact counts; 512 products (learned +
+# batched against 512 plain calls, with the HLL- and
 # exact-sized batched forms beside it, on the device and end to end).
 
 def _ev():
@@ -788,7 +788,7 @@ def leg_small(name: str, stream, steps: int = 20, warmup: int = 5, check: bool =
 
 
 def leg_sizing(stream, steps: int = 3, warmup: int = 2) -> dict:
-    """Config 4: row sizes of C = A*A for the held-out R-MAT n = 2^21 (24 per
+    """Row sizes of C = A*A for the held-out R-MAT n = 2^21 (24 per
     row, seed 7; generated on the device; C, ~0.55 TB, is never formed) by
     exact symbolic counts, HLL and the learned network, with the estimates'
     errors against the exact counts on the rows they size (> 128 products)."""
@@ -814,7 +814,7 @@ def leg_sizing(stream, steps: int = 3, warmup: int = 2) -> dict:
 
 def leg_batch(stream, steps: int = 3, warmup: int = 2, e2e_steps: int = 2, ablation: bool = True,
               check: bool = True) -> dict:
-    """Config 5: 512 independent A_p*A_p (n log-uniform 1k-64k; banded, R-MAT,
+    """512 independent A_p*A_p (n log-uniform 1k-64k; banded, R-MAT,
     uniform and block-diagonal in turn; 4-32 entries per row; FP64; generated
     on the device, seed 5). Plain: 512 sequential ocean_spgemm calls. Learned +
     batched: one captured graph of the whole batch, rows sized by the network,
@@ -1040,7 +1040,7 @@ def release_memory():
 
 
 def run_batch(args, world, rank, local):
-    """Workload batch512 alone (config 5): see leg_batch."""
+    """Workload batch512 alone: see leg_batch."""
     import torch
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
@@ -1062,7 +1062,7 @@ def run_batch(args, world, rank, local):
 
 
 def run_sizing(args, world, rank, local):
-    """Workload rmat21-sizing alone (config 4): see leg_sizing."""
+    """Workload rmat21-sizing alone: see leg_sizing."""
     import torch
     torch.cuda.set_device(local)
     r = leg_sizing(torch.cuda.current_stream(), steps=args.steps, warmup=args.warmup)

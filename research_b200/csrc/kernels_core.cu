@@ -2589,8 +2589,8 @@ int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const 
   const uint64_t per_block = 256 / g;
   const unsigned blocks = (unsigned)((A.rows + per_block - 1) / per_block);
   int launched = 0;
-  // the row table of B pays from about a million entries of B (config 1,
-  // 0.33 M entries: its extra launch costs more than it saves)
+  // the row table of B pays from about a million entries of B (on the 256x256
+  // Laplacian, 0.33 M entries, its extra launch costs more than it saves)
   const uint4* btab = (w.btab && B.nnz >= (1ull << 20)) ? w.btab : nullptr;
   if (btab) {
     k_brow_table<RP><<<(unsigned)std::min<uint64_t>((B.rows + 255) / 256, 148ull * 16), 256, 0, s>>>(B, w.btab);

@@ -2,8 +2,8 @@
 most 256 products) in registers or shared memory, finds its tile's output
 offset by a decoupled look-back and writes C in place. Checked against the CPU
 oracle (structure bit for bit, values within 1e-12 * sum |a*b|) on the
-Laplacian 256^2 (config 1), the rectangular A*A^T (config 3, rows up to 131
-products: the shared-memory sort path), rows at every product-count boundary
+Laplacian 256^2, the rectangular A*A^T (rows up to 131 products: the
+shared-memory sort path), rows at every product-count boundary
 (0, 1, 32, 33, 64, 65, 128, 129, 256), the last tile partly filled, forced
 64-bit output row pointers, and inputs the fused path does not take (a row
 over 256 products; fused_ultrasparse off), which must give the same C."""
