@@ -143,19 +143,23 @@ __global__ void __launch_bounds__(256) k_brow_table(Csr<RP> B, uint4* __restrict
 // Products, smallest first column, largest last column and longest B row
 // over A entries k0, k0 + G, k0 + 2G, ... below k1, accumulated into p, mn,
 // mx, lb. Four entries per pass have their dependent loads in flight together;
-// with the row table of B (btab) each entry is one table load.
+// with the row table of B (btab) each entry is one table load, two per pass.
 template <int G, typename RP>
 __device__ __forceinline__ void span_part(const Csr<RP>& A, const Csr<RP>& B, const uint4* __restrict__ btab,
                                           uint64_t k0, uint64_t k1, unsigned long long& p, uint32_t& mn,
                                           uint32_t& mx, uint32_t& lb) {
   if (btab) {
-    for (; k0 < k1; k0 += 4 * G) {
-      uint4 t[4];
+    // two table loads in flight: with 32 registers k_analysis keeps 8 blocks
+    // per SM (6 with 64-bit row pointers), which hides the block barriers'
+    // wait for each block's slowest row (held-out R-MAT 2^21 learned sizing
+    // 2.77 -> 2.34 ms against 4 entries in flight at 61 registers)
+    for (; k0 < k1; k0 += 2 * G) {
+      uint4 t[2];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < 2; ++u)
         t[u] = k0 + (uint64_t)u * G < k1 ? btab[A.col[k0 + (uint64_t)u * G]] : make_uint4(kEmpty, 0u, 0u, 0u);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 2; ++u) {
         const uint64_t len = (uint64_t)t[u].z | ((uint64_t)t[u].w << 32);
         if (len) {
           p += len;
@@ -220,7 +224,7 @@ __device__ __forceinline__ int analysis_write(uint64_t row, uint64_t a_len, unsi
 // Rows longer than kLongRowEntries are only listed here (when the list
 // exists) and summarised by k_analysis_long.
 template <typename RP, int G>
-__global__ void __launch_bounds__(256) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
+__global__ void __launch_bounds__(256, sizeof(RP) == 4 ? 8 : 6) k_analysis(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
                                                   uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
                                                   uint32_t* __restrict__ anz, uint32_t* __restrict__ maxb,
                                                   uint32_t* __restrict__ row_nnz, uint64_t* __restrict__ bm_off,
