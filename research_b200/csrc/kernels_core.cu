@@ -352,12 +352,16 @@ __global__ void __launch_bounds__(256, sizeof(RP) == 4 ? 8 : 6) k_analysis(Csr<R
   }
 }
 
+// Grid of the long-row kernels: 8 blocks of 256 per SM (32 registers), so
+// enough chunks are in flight to hide their atomics and fences.
+constexpr unsigned kLongGrid = 8 * 148;
+
 // The analysis of the listed long rows: the warps of the grid stride over the
 // chunk ids, merge each chunk's partial sums into its row's accumulator with
 // atomics, and the warp that finishes a row's last chunk writes the row's
 // results, appends it to its class and adds its totals.
 template <typename RP>
-__global__ void __launch_bounds__(256) k_analysis_long(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
+__global__ void __launch_bounds__(256, 8) k_analysis_long(Csr<RP> A, Csr<RP> B, uint32_t* __restrict__ prod,
                                                        uint32_t* __restrict__ lo, uint32_t* __restrict__ hi,
                                                        uint32_t* __restrict__ anz, uint32_t* __restrict__ maxb,
                                                        uint32_t* __restrict__ row_nnz,
@@ -2354,7 +2358,7 @@ __global__ void __launch_bounds__(256) k_hll_estimate(Csr<RP> A, const uint8_t* 
 // row's registers with per-register atomicMax, and the warp that finishes the
 // row's last chunk computes the row's estimate.
 template <typename RP, int LOGP>
-__global__ void __launch_bounds__(256) k_hll_estimate_long(Csr<RP> A, const uint8_t* __restrict__ sk,
+__global__ void __launch_bounds__(256, 8) k_hll_estimate_long(Csr<RP> A, const uint8_t* __restrict__ sk,
                                                            const uint32_t* __restrict__ prod,
                                                            const uint32_t* __restrict__ lo,
                                                            const uint32_t* __restrict__ hi,
@@ -2611,7 +2615,7 @@ int launch_analysis(const Csr<RP>& A, const Csr<RP>& B, const DevWork& w, const 
 #undef OCEAN_ANALYSIS
   ++launched;
   if (w.long_acc) {
-    k_analysis_long<RP><<<4 * 148, 256, 0, s>>>(A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off,
+    k_analysis_long<RP><<<kLongGrid, 256, 0, s>>>(A, B, w.prod, w.lo, w.hi, w.anz, w.maxb, w.row_nnz, w.bm_off,
                                                 w.sym_bins, w.ctr, pols, row_pol, w.long_rows, w.long_acc, w.long_cap,
                                                 w.long_chunk_row, w.long_chunk_cap, btab);
     ++launched;
@@ -2835,11 +2839,11 @@ int launch_hll_rows(const Csr<RP>& A, const DevWork& w, int log2p, double expans
     k_hll_estimate<RP, 6><<<ga, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro, w.long_acc);
   if (!w.long_acc) return 1;
   if (log2p == 5)
-    k_hll_estimate_long<RP, 5><<<4 * 148, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro,
+    k_hll_estimate_long<RP, 5><<<kLongGrid, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro,
                                                        w.ctr, w.long_rows, w.long_acc, w.long_cap,
                                                        w.long_chunk_row, w.long_chunk_cap);
   else
-    k_hll_estimate_long<RP, 6><<<4 * 148, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro,
+    k_hll_estimate_long<RP, 6><<<kLongGrid, 256, 0, s>>>(A, sketch, w.prod, w.lo, w.hi, out, expansion, esc_max, ro,
                                                        w.ctr, w.long_rows, w.long_acc, w.long_cap,
                                                        w.long_chunk_row, w.long_chunk_cap);
   return 2;
