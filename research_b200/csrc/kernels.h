@@ -63,7 +63,7 @@ struct DevWork {
   const uint8_t* row_pol = nullptr;
 };
 
-constexpr int kScanTile = 4096;
+constexpr int kScanTile = 1024;  // rows per scan tile: 1024 threads of k_scan_reduce, 256 x 4 of k_scan_apply
 inline uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
 
 // Class choice of a row (tunable: the batched autotuner searches these).

@@ -2093,9 +2093,11 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(unsigned long long* __restr
   }
 }
 
-// Per tile: local exclusive scan + tile offset -> row pointers; each row is
-// also appended to its numeric class list.
-__global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict__ in, uint64_t n,
+// Per tile (256 threads x 4 rows): local exclusive scan + tile offset -> row
+// pointers; each row is also appended to its numeric class list.
+constexpr int kScanApplyThreads = kScanTile / 4;
+static_assert(NB_COUNT * kMaxChunks <= kScanApplyThreads, "one thread per class-list counter");
+__global__ void __launch_bounds__(kScanApplyThreads) k_scan_apply(const uint32_t* __restrict__ in, uint64_t n,
                                                      const unsigned long long* __restrict__ tile_offs,
                                                      uint64_t* __restrict__ rowptr64,
                                                      uint32_t* __restrict__ rowptr32,
@@ -2126,7 +2128,8 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const uint32_t* __restrict_
     s += v[q];
   }
   unsigned long long total;
-  unsigned long long run = block_excl_scan<1024, unsigned long long>(s, scr, &total) + tile_offs[blockIdx.x];
+  unsigned long long run =
+      block_excl_scan<kScanApplyThreads, unsigned long long>(s, scr, &total) + tile_offs[blockIdx.x];
   int bq[4], sq[4];
   uint32_t rq[4], aq[4], pq[4];
 #pragma unroll
@@ -2688,7 +2691,7 @@ int launch_scan(const DevWork& w, const uint32_t* in, uint64_t* out64, uint32_t*
   k_scan_reduce<<<(unsigned)nt, 1024, 0, s>>>(in, w.rows, w.tile_sums);
   k_scan_tiles<<<1, 1024, 0, s>>>(w.tile_sums, nt, total, out64, out32, w.rows);
   const int chunks = bin_rows ? w.chunks : 0;
-  k_scan_apply<<<(unsigned)nt, 1024, 0, s>>>(in, w.rows, w.tile_sums, out64, out32, w.prod, w.lo, w.hi, w.anz,
+  k_scan_apply<<<(unsigned)nt, kScanApplyThreads, 0, s>>>(in, w.rows, w.tile_sums, out64, out32, w.prod, w.lo, w.hi, w.anz,
                                              w.bm_off, w.num_bins, w.ctr, pols, row_pol, bin_rows ? 1 : 0, chunks,
                                              w.chunk_bound, w.chunk_count);
   return 3;
