@@ -714,19 +714,25 @@ def _ev():
     return torch.cuda.Event(enable_timing=True)
 
 
-def time_on_device(fn, steps: int, warmup: int, stream) -> float:
-    """Mean ms per call of fn() over `steps` calls after `warmup`, CUDA events on `stream`."""
+def time_on_device(fn, steps: int, warmup: int, stream, reps: int = 1) -> float:
+    """Mean ms per call of fn() over `steps` calls after `warmup`, CUDA events on
+    `stream`; with reps > 1 the median of that many such means (the forms that
+    read counters back to the host between their launches are exposed to host
+    scheduling stalls, which a median of repeated means does not carry)."""
     import torch
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
-    e0, e1 = _ev(), _ev()
-    e0.record(stream)
-    for _ in range(steps):
-        fn()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / steps
+    means = []
+    for _ in range(max(1, reps)):
+        e0, e1 = _ev(), _ev()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        means.append(e0.elapsed_time(e1) / steps)
+    return float(np.median(means))
 
 
 def leg_small(name: str, stream, steps: int = 20, warmup: int = 5, check: bool = True) -> dict:
@@ -738,12 +744,13 @@ def leg_small(name: str, stream, steps: int = 20, warmup: int = 5, check: bool =
     dA = DeviceCSR.from_host(A)
     dB = dA if same else DeviceCSR.from_host(B)
     g = SpGEMM({})
-    plain_ms = time_on_device(lambda: g.multiply(dA, dB, sptr).free(sptr), steps, warmup, stream)
+    plain_ms = time_on_device(lambda: g.multiply(dA, dB, sptr).free(sptr), steps, warmup, stream, reps=5)
     st = g.get_stats()
     products, nnz_c = int(st["stats"]["intermediate_product"]), int(st["C"]["nnz"])
     out = {"workload": desc, "products": products, "nnz_C": nnz_c, "workflow": st["decision"]["workflow"],
            "plain_ms": round(plain_ms, 4), "plain_gflops": round(2.0 * products / plain_ms / 1e6, 3),
-           "kernel_launches": st["decision"]["kernel_launches"]}
+           "kernel_launches": st["decision"]["kernel_launches"],
+           "timing": f"median of 5 means of {steps} calls each (CUDA events on the launching stream)"}
     if check:
         from oracle import oracle as O
         C = g.multiply(dA, dB, sptr)
@@ -753,7 +760,7 @@ def leg_small(name: str, stream, steps: int = 20, warmup: int = 5, check: bool =
         out["parity_max_rel_err"] = O.compare(h.rowptr, h.col, h.val, cp, cj, cx, ca, 1e-12)
     gb = SpGEMM({})
     plan = Batch(gb, [dA], [dB], sptr)
-    plan_ms = time_on_device(lambda: plan.launch(sptr), steps, warmup, stream)
+    plan_ms = time_on_device(lambda: plan.launch(sptr), steps, warmup, stream, reps=5)
     out["captured_plan_ms"] = round(plan_ms, 4)
     out["captured_plan_launches"] = plan.info()["kernel_launches"]
     plan.close()
@@ -773,7 +780,7 @@ def leg_small(name: str, stream, steps: int = 20, warmup: int = 5, check: bool =
     res = CsrOut()
     e2e_ms = time_on_device(lambda: _check(lib().ocean_spgemm_host(g._h, ctypes.byref(av), ctypes.byref(bv),
                                                                    ctypes.byref(res), sptr)),
-                            steps, warmup, stream)
+                            steps, warmup, stream, reps=5)
     out["e2e_ms"] = round(e2e_ms, 4)
     out["e2e_gflops"] = round(2.0 * products / e2e_ms / 1e6, 3)
     g.close()
@@ -839,11 +846,12 @@ def leg_batch(stream, steps: int = 3, warmup: int = 2, e2e_steps: int = 2, ablat
     def plain_step():
         for a in dA:
             gp.multiply(a, a, sptr).free(sptr)
-    plain_ms = time_on_device(plain_step, steps, warmup, stream)
+    plain_ms = time_on_device(plain_step, 1, warmup, stream, reps=max(3, steps))
     gf = lambda ms: round(2.0 * products / (ms / 1e3) / 1e9, 3)
     out = {"workload": "512 x A_p*A_p, n log-uniform 1k-64k, banded/R-MAT/uniform/block-diagonal in turn, "
                        "4-32 entries per row, FP64 U[-1,1], seed 5", "products": products,
-           "plain": {"ms": round(plain_ms, 3), "gflops": gf(plain_ms), "form": "512 sequential ocean_spgemm calls"}}
+           "plain": {"ms": round(plain_ms, 3), "gflops": gf(plain_ms),
+                     "form": f"512 sequential ocean_spgemm calls; median of {max(3, steps)} such steps"}}
 
     def batched(config):
         gb = SpGEMM(config)
