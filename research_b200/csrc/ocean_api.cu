@@ -149,6 +149,7 @@ struct ocean_handle {
   Config cfg;
   int device = 0;
   int num_sms = 148;
+  uint64_t device_bytes = 0;  // total device memory (read once at creation)
   DevWork w;
   uint64_t cap_rows = 0;
   DevCounters* h_ctr = nullptr;  // pinned
@@ -255,6 +256,11 @@ void init_handle(ocean_handle* h, const std::string& json) {
   h->cfg = Config::from_json_text(json);
   OCEAN_CUDA(cudaGetDevice(&h->device));
   OCEAN_CUDA(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+  {
+    size_t free_b = 0, total_b = 0;
+    OCEAN_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    h->device_bytes = total_b;
+  }
   // Stream-ordered allocations come from the device's default pool, which is told
   // to keep freed memory (as the reference does, kernels/SpGEMM.cuh:219-223).
   cudaMemPool_t pool;
@@ -448,6 +454,15 @@ uint64_t available_device_bytes(int device) {
     cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
   }
   return (uint64_t)free_b + (reserved > used ? reserved - used : 0);
+}
+
+// Whether `bytes` fit in `frac` of the memory the device can still give.
+// Needs below 1% of the device's memory are taken to fit without asking: the
+// driver query costs tens of microseconds, as much as the whole analysis of
+// a problem that small, and an allocation that fails still raises an error.
+bool fits_device(const ocean_handle* h, double bytes, double frac) {
+  if (bytes < 0.01 * (double)h->device_bytes) return true;
+  return bytes < frac * (double)available_device_bytes(h->device);
 }
 
 // Policies of the class choice from the config.
@@ -789,7 +804,7 @@ int choose_workflow(ocean_handle* h, const Csr<RP>& A, const Csr<RP>& B, cudaStr
   if (c.force_workflow == WF_ULTRASPARSE ||
       (c.force_workflow < 0 && c.use_ultrasparse_workflow && A.rows &&
        (double)products / (double)A.rows <= c.usparse_avg_product_threshold &&
-       12.0 * (double)products < 0.4 * (double)available_device_bytes(h->device))) {
+       fits_device(h, 12.0 * (double)products, 0.4))) {
     OCEAN_CUDA(cudaMemcpyAsync(h->w.est, h->w.prod, A.rows * 4, cudaMemcpyDeviceToDevice, s));
     return WF_ULTRASPARSE;
   }
@@ -1040,7 +1055,7 @@ void run_spgemm(ocean_handle* h, const ocean_csr_view* Av, const ocean_csr_view*
         OCEAN_CUDA(cudaMemcpyAsync(h->h_ctr, h->w.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
         OCEAN_CUDA(wait_stream(s, h->cfg.spin_wait_us));
         st.total_est = h->h_ctr->total_est;
-        if (12.0 * (double)st.total_est > 0.45 * (double)available_device_bytes(h->device)) {
+        if (!fits_device(h, 12.0 * (double)st.total_est, 0.45)) {
           wf = WF_PRECISE;  // the temporary output would not fit: count exactly instead
           OCEAN_CUDA(cudaMemsetAsync(h->w.ctr->num_count, 0, sizeof(unsigned) * NB_COUNT * 2, s));
         }
